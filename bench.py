@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Throughput of the fused FP32 shallow-water step on B200.
+
+Metric: Mcell-updates/s (one cell-update = one full RK2 step of one cell,
+friction included) and its fraction of the HBM roofline.
+
+Workload: the runup scenario (plane beach + 20 seeded Gaussian bumps, west
+water-level inflow from a leading-depression N-wave, walls elsewhere,
+Manning n = 0.01, dx = 0.014 m) tiled to 4096 x 4096 cells; synthetic data.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1).  Each rank steps its own replica of
+the grid -- the single-grid step has no exchange (weak scaling) -- and rank 0
+prints one JSON line.  ``value`` is device-timed with CUDA events around K
+steps with inputs resident in HBM; ``e2e`` is the same metric through the
+public ``SWE2D.forward`` call with the state copied from pinned host memory
+and back inside the timed region.  ``--impl reference`` times the CPU oracle
+(a C restatement of the reference step, all host threads) on a bounded crop
+of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+BYTES_PER_CELL_UPDATE = 32  # read h,hu,hv,z,n once, write h,hu,hv once
+STAGE2_BYTES_PER_CELL = 44  # stage-2 kernel: read U, k1, z, n; write U
+L2_BYTES = 126 * 2 ** 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--ny", type=int, default=4096)
+    ap.add_argument("--nx", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def workload(ny, nx):
+    from diffswe2d_b200 import scenarios
+    base = scenarios.runup(seed=0)
+    return scenarios.tiled(base, ny, nx)
+
+
+def level_at(sc, t: float) -> float:
+    """Float32 linear interpolation of the west boundary series at time t."""
+    times, levels = sc.bc_times, sc.bc_levels
+    i = int(np.searchsorted(times, np.float32(t), side="left"))
+    i = min(max(i, 1), len(times) - 1)
+    w = (np.float32(t) - times[i - 1]) / max(times[i] - times[i - 1], np.float32(1.1920929e-07))
+    return float(levels[i - 1] + np.float32(w) * (levels[i] - levels[i - 1]))
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(sc, max_seconds=12.0, crop=1024):
+    """The CPU oracle (C restatement, all host threads) on a crop of the workload."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import OracleSWE, num_threads
+    from diffswe2d_b200.config import SWEConfig
+    bed = sc.bed[:crop, :crop]
+    m = OracleSWE(bed, sc.roughness[:crop, :crop], sc.dx, sc.dy, SWEConfig(**sc.config))
+    U = np.ascontiguousarray(sc.U0[:, :, :crop, :crop])
+    U, _ = m.step(U, 0.0, 1.0e9, boundary_level=level_at(sc, 0.0))  # warm caches
+    steps, t0, t = 0, time.perf_counter(), 0.0
+    while True:
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        t += dt
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or steps >= 200:
+            break
+    cells = bed.size
+    return {"value": cells * steps / el / 1e6, "unit": "Mcell-updates/s", "cores": num_threads(),
+            "kind": "port",
+            "sample": f"{steps} steps of a {crop}x{crop} crop of the workload ({el:.1f} s)"}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU oracle port of the reference step, rank 0 only."""
+    if rank != 0:
+        return
+    sc = workload(args.ny, args.nx)
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import OracleSWE, num_threads
+    from diffswe2d_b200.config import SWEConfig
+    crop = 1024
+    m = OracleSWE(sc.bed[:crop, :crop], sc.roughness[:crop, :crop], sc.dx, sc.dy,
+                  SWEConfig(**sc.config))
+    U = np.ascontiguousarray(sc.U0[:, :, :crop, :crop])
+    t = 0.0
+    for _ in range(args.warmup):
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        t += dt
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        t += dt
+    el = time.perf_counter() - t0
+    value = crop * crop * args.steps / el / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcell-updates/s & %HBM peak", "value": value,
+        "unit": "Mcell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"runup_tiled_{args.ny}x{args.nx}", "sample": f"{crop}x{crop} crop",
+                   "dx": sc.dx},
+        "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": num_threads(),
+                         "kind": "port",
+                         "sample": f"{args.steps} steps of a {crop}x{crop} crop of the workload"},
+        "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from diffswe2d_b200 import SWE2D, SWEConfig
+    from diffswe2d_b200 import _native as nat
+
+    sc = workload(args.ny, args.nx)
+    ny, nx = sc.bed.shape
+    cells = ny * nx
+    cfg = SWEConfig(**sc.config)
+    model = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev),
+                  sc.dx, sc.dy, config=cfg, train_dem=False)
+    model.set_dynamic_boundary(torch.from_numpy(sc.bc_times).to(dev),
+                               torch.from_numpy(sc.bc_levels).to(dev))
+    lib = nat.lib()
+    p = nat.params(cfg, sc.dx, sc.dy)
+    bed = model.bed.detach().contiguous()
+    n = model.roughness_length.contiguous()
+    U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]
+    k1 = torch.empty_like(U[0])
+    red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+    stream = nat.stream_handle(dev)
+    # Host-side replica of the model time so every step sees the inflow level of
+    # its own time; the levels are staged on the device before the timed region.
+    total = args.warmup + args.steps
+    levels_host, t = [], 0.0
+    dt_probe = None
+    lev = torch.zeros(total, dtype=torch.float32, device=dev)
+
+    def launch(i, src, dst, stage):
+        rc = lib.swe_step_stage_f32(stage, nat.ptr(src), nat.ptr(bed), 1, nat.ptr(n), 1, 1, ny, nx, p,
+                                    ctypes.c_void_p(lev.data_ptr() + 4 * i), 1, 1.0e9, None, 0, 1,
+                                    nat.ptr(k1), nat.ptr(red), nat.ptr(dst), stream)
+        nat.check(rc, "step")
+
+    # The CFL time step of this workload barely changes over a few hundred
+    # steps; one probe step fixes the schedule of inflow levels.
+    launch(0, U[0], U[1], 3)
+    dt_probe = float(red[3:4].view(torch.float32).item())
+    for i in range(total):
+        levels_host.append(level_at(sc, t))
+        t += dt_probe
+    lev.copy_(torch.tensor(levels_host, dtype=torch.float32))
+
+    src = 0
+    for i in range(args.warmup):
+        launch(i, U[src], U[1 - src], 3)
+        src = 1 - src
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with Clocks(local) as clk:
+        ev[0].record()
+        for k in range(args.steps):
+            i = args.warmup + k
+            launch(i, U[src], U[1 - src], 1)
+            ev[2 * k + 1].record()
+            launch(i, U[src], U[1 - src], 2)
+            ev[2 * k + 2].record()
+            src = 1 - src
+        torch.cuda.synchronize(dev)
+    total_ms = ev[0].elapsed_time(ev[-1])
+    s1 = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+    s2 = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)]
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
+    status = int(red[2].item())
+    finite = bool(torch.isfinite(U[src]).all().item())
+
+    # End to end: SWE2D.forward through the public API with the state copied
+    # in from pinned host memory and back out every step.
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(sc.U0).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        chunk = 20 * dt_probe  # about 20 internal CFL steps per call
+        counts = []
+        e2e_steps = 3
+        for w in range(2):  # warm-up
+            Ud = host_in.to(dev, non_blocking=True)
+            Uf, _ = model(Ud, t_end=chunk, start_time=0.0)
+            host_out.copy_(Uf, non_blocking=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(e2e_steps):
+            c = []
+            Ud = host_in.to(dev, non_blocking=True)
+            Uf, _ = model(Ud, t_end=chunk, start_time=0.0, callback=lambda it, tt, UU: c.append(it))
+            host_out.copy_(Uf, non_blocking=True)
+            counts.append(len(c))
+        e1.record()
+        torch.cuda.synchronize(dev)
+        e2e_ms = e0.elapsed_time(e1)
+        if world > 1:
+            tt = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_ms = float(tt.item())
+        nbytes = host_in.numel() * 4
+        e2e = {"value": world * cells * sum(counts) / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "api": "SWE2D.forward(U0 from pinned host, t_end=~20 CFL steps) + state back to host",
+               "internal_steps_per_call": counts}
+
+    peak, peak_kind = measured_peaks()
+    s2_avg = statistics.mean(s2)
+    s1_avg = statistics.mean(s1)
+    achieved = STAGE2_BYTES_PER_CELL * cells / (s2_avg * 1e-3) / 1e9
+    step_achieved = BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
+    line = {
+        "metric": "Mcell-updates/s & %HBM peak",
+        "value": value,
+        "unit": "Mcell-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"runup_tiled_{ny}x{nx}", "grid": [ny, nx], "dx": sc.dx,
+                   "boundaries": "west water_level (N-wave), walls", "manning": 0.01,
+                   "l2": "inputs larger than L2: state 201 MB + k1 201 MB + bed/n 134 MB per replica",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "stage2 (predictor+tendency+corrector+friction)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "bytes_per_cell": STAGE2_BYTES_PER_CELL,
+                     "stage1_ms": s1_avg, "stage2_ms": s2_avg,
+                     "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak,
+                     "step_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "status_word": status,
+        "state_finite": finite,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

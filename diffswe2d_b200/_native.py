@@ -1,0 +1,137 @@
+"""ctypes binding of libswe_b200.so, the sm_100a kernels behind the C ABI
+declared in ``include/swe_b200.h``.
+
+There is no fallback: if the library is missing, or a tensor is not a
+contiguous float32 CUDA tensor, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libswe_b200.so"
+
+SWE_OK, SWE_EARG, SWE_ECUDA = 0, 1, 2
+S_NONFINITE_STATE, S_NONFINITE_DT, S_NONPOSITIVE_DT = 1, 2, 4
+RED_WORDS = 8
+FORCING_NONE, FORCING_SCALAR, FORCING_FIELD = 0, 1, 2
+
+BC_CODES = {
+    "transmissive": 0,
+    "periodic": 1,
+    "constant": 2,
+    "water_level": 3,
+    "wall": 4,
+    "absorbing": 5,
+}
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library is missing or a call into it failed."""
+
+
+class SweParams(ctypes.Structure):
+    _fields_ = [
+        ("gravity", ctypes.c_double),
+        ("dry_depth", ctypes.c_double),
+        ("epsilon", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("theta", ctypes.c_double),
+        ("dx", ctypes.c_double),
+        ("dy", ctypes.c_double),
+        ("constant_value", ctypes.c_double),
+        ("bc_left", ctypes.c_int32),
+        ("bc_right", ctypes.c_int32),
+        ("bc_top", ctypes.c_int32),
+        ("bc_bottom", ctypes.c_int32),
+        ("water_slope_reset", ctypes.c_int32),
+        ("positivity_limiter", ctypes.c_int32),
+        ("apply_friction", ctypes.c_int32),
+        ("friction_model", ctypes.c_int32),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+# name -> argtypes, in the order of include/swe_b200.h
+_SIGNATURES = {
+    "swe_spatial_operator_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
+                                 _P, _I, _I, _P, _I, _I, _P, _P, _P],
+    "swe_step_f32": [_P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _F,
+                     _P, _I, _I, _P, _P, _P, _P],
+    "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
+                           _F, _P, _I, _I, _P, _P, _P, _P],
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the library once; raise NativeLibraryError if it is absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise NativeLibraryError(
+                f"{LIB_PATH} is missing; build it with `make -C diffswe2d_b200/csrc` "
+                "(or __graft_entry__.build())")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, args in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        _lib = handle
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGNATURES)
+
+
+def params(cfg, dx: float, dy: float) -> SweParams:
+    for side in ("left", "right", "top", "bottom"):
+        name = getattr(cfg, f"boundary_{side}")
+        if name not in BC_CODES:
+            raise ValueError(f"Unsupported {side} boundary type {name!r}. "
+                             f"Valid types are {sorted(BC_CODES)}.")
+    if cfg.frictionmodel not in ("manning", "roughness_length") and cfg.apply_friction:
+        # The reference treats every name other than "manning" as roughness length.
+        pass
+    return SweParams(
+        float(cfg.gravity), float(cfg.dry_depth), float(cfg.epsilon), float(cfg.cfl),
+        float(cfg.limiter_theta), float(dx), float(dy), float(cfg.constant_value),
+        BC_CODES[cfg.boundary_left], BC_CODES[cfg.boundary_right],
+        BC_CODES[cfg.boundary_top], BC_CODES[cfg.boundary_bottom],
+        int(bool(cfg.water_slope_reset)), int(bool(cfg.positivity_limiter)),
+        int(bool(cfg.apply_friction)), 0 if cfg.frictionmodel == "manning" else 1,
+    )
+
+
+def require_cuda_f32(name: str, t: torch.Tensor) -> torch.Tensor:
+    if not torch.is_tensor(t):
+        raise TypeError(f"{name} must be a tensor")
+    if not t.is_cuda:
+        raise NativeLibraryError(
+            f"{name} is on {t.device}; the B200 kernels only run on CUDA tensors")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name} must be float32 for the FP32 kernels, got {t.dtype}")
+    return t.contiguous()
+
+
+def stream_handle(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def check(rc: int, what: str) -> None:
+    if rc == SWE_OK:
+        return
+    if rc == SWE_EARG:
+        raise ValueError(f"{what}: invalid argument rejected by the CUDA library")
+    raise NativeLibraryError(f"{what}: CUDA error (code {rc})")

@@ -1,0 +1,343 @@
+// swe_math.cuh -- FP32 arithmetic of the DiffSWE2d finite-volume step.
+//
+// Every function evaluates the same expression tree, in the same order and
+// with the same rounding points, as the PyTorch code it cites (paths are
+// relative to the DiffSWE2d project).  The file is compiled with
+// -fmad=false -prec-div=true -prec-sqrt=true -ftz=false, so each +,-,*,/
+// and sqrt is one IEEE correctly-rounded operation: the results are those of
+// the reference's float32 tensors op for op.
+//
+// Python scalars that the reference multiplies into float32 tensors are
+// rounded to float32 first (PyTorch casts a wrapped scalar to the tensor's
+// dtype); they arrive pre-rounded in SweConsts.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define SWE_HD __host__ __device__ __forceinline__
+#else
+#define SWE_HD inline
+#endif
+
+namespace swe {
+
+// Constants of one configuration, rounded to float32 as the reference rounds
+// them at each use.
+struct SweConsts {
+    float g;          // float(gravity)                  riemann.py:36, :76
+    float half_g;     // 0.5 * gravity                    reconstruction.py:101, riemann.py:76
+    float dry;        // dry_depth                        riemann.py:29
+    float floor_h;    // max(eps, dry, 1e-6)              riemann.py:6-11, reconstruction.py:12-15
+    float den_floor;  // max(eps, 1e-6)                   riemann.py:14-17
+    float theta;      // limiter_theta                    numerics.py:27
+    float eps;        // epsilon                          solver.py:552, :621
+    float cfl;        // cfl                              solver.py:623
+    float dx, dy;     // grid spacing                     solver.py:514, :518
+    float fr_vs;      // friction _floor(h, eps, dry)     friction.py:17
+    float fr_e;       // friction _floor(h, eps)          friction.py:63
+    float fr_e2;      // _floor(h, eps) ** 2              friction.py:27
+    float third;      // 1.0 / 3.0                        friction.py:66
+    float absorb_lim; // 1e-4                             boundary.py:325
+    float absorb_min; // 1e-6                             boundary.py:326
+    float g981;       // 9.81 (hard-coded)                friction.py:66, boundary.py:326
+    float wall_pad0, wall_pad1;  // unused padding, keeps 16-byte multiples
+};
+
+// ---------------------------------------------------------------- numerics
+// minmod3, numerics.py:4-13.  With lo = min(a,b,c) and hi = max(a,b,c):
+// all three positive <=> lo > 0, and then sign(a)*min|.| = lo exactly; all
+// negative <=> hi < 0, and then the result is -min(-a,-b,-c) = hi exactly;
+// any zero or mixed signs gives 0.
+SWE_HD float minmod3(float a, float b, float c) {
+    float lo = fminf(a, fminf(b, c));
+    float hi = fmaxf(a, fmaxf(b, c));
+    return lo > 0.0f ? lo : (hi < 0.0f ? hi : 0.0f);
+}
+
+// limited_increment, numerics.py:16-27, for a cell with neighbours qm, qp.
+SWE_HD float limited_increment(float qm, float q, float qp, float theta) {
+    float backward = q - qm;
+    float centred = 0.5f * (qp - qm);
+    float forward = qp - q;
+    return minmod3(theta * backward, centred, theta * forward);
+}
+
+// Per-cell primitive values (riemann.py:20-38) plus eta = h + bed
+// (reconstruction.py:23-24).
+struct Prim {
+    float h, u, v, eta, z;
+};
+
+SWE_HD Prim make_prim(float U0, float U1, float U2, float z, const SweConsts& k) {
+    Prim p;
+    p.h = fmaxf(U0, 0.0f);
+    bool wet = p.h > k.dry;
+    float safe = fmaxf(p.h, k.floor_h);
+    p.u = wet ? U1 / safe : 0.0f;
+    p.v = wet ? U2 / safe : 0.0f;
+    p.eta = p.h + z;
+    p.z = z;
+    return p;
+}
+
+// Face-side values a cell contributes to the two faces across it in one
+// direction (reconstruction.py:26-96).  "p" is the side facing +direction
+// (the left state UL of the face k+1/2), "m" the side facing -direction (the
+// right state UR of the face k-1/2).
+struct Side {
+    float hlin;  // h +/- 0.5 dh
+    float eta;   // eta +/- 0.5 deta
+    float bed;   // z +/- 0.5 dz
+    float u, v;  // u +/- 0.5 factor du
+};
+
+struct Sides {
+    Side p, m;
+    float h, z;  // cell depth and bed for the well-balanced sources
+};
+
+// c is the cell, a its neighbour in -direction, b in +direction.
+SWE_HD Sides make_sides(const Prim& a, const Prim& c, const Prim& b, const SweConsts& k,
+                        bool water_slope_reset) {
+    float dh = limited_increment(a.h, c.h, b.h, k.theta);        // :26
+    float deta = limited_increment(a.eta, c.eta, b.eta, k.theta); // :27
+    float dz = limited_increment(a.z, c.z, b.z, k.theta);        // :28
+    float du = limited_increment(a.u, c.u, b.u, k.theta);        // :29
+    float dv = limited_increment(a.v, c.v, b.v, k.theta);        // :30
+    if (water_slope_reset) {                                     // :32-42
+        float half = 0.5f * (deta - dh);
+        float base = c.eta - c.h;
+        float bed_minus = base - half;
+        float bed_plus = base + half;
+        bool reset = (deta * deta > dz * dz) && ((bed_minus > a.eta) || (bed_plus > b.eta));
+        if (reset) deta = dh + dz;
+    }
+    Sides s;
+    float hdh = 0.5f * dh, hdeta = 0.5f * deta, hdz = 0.5f * dz;
+    s.p.hlin = c.h + hdh;   // :50
+    s.m.hlin = c.h - hdh;   // :51
+    s.p.eta = c.eta + hdeta;  // :53
+    s.m.eta = c.eta - hdeta;  // :54
+    s.p.bed = c.z + hdz;    // :56
+    s.m.bed = c.z - hdz;    // :57
+    float safe = fmaxf(c.h, k.floor_h);  // :71-73
+    float q = hdh / safe;                // 0.5 * dh / safe_h, :75-76
+    bool wet = c.h > k.dry;              // :78-87
+    float fL = wet ? 1.0f - q : 1.0f;
+    float fR = wet ? 1.0f + q : 1.0f;
+    fL = fminf(fmaxf(fL, -10.0f), 10.0f);  // :90-91
+    fR = fminf(fmaxf(fR, -10.0f), 10.0f);
+    float hfL = 0.5f * fL, hfR = 0.5f * fR;
+    s.p.u = c.u + hfL * du;  // :93-96
+    s.p.v = c.v + hfL * dv;
+    s.m.u = c.u - hfR * du;
+    s.m.v = c.v - hfR * dv;
+    s.h = c.h;
+    s.z = c.z;
+    return s;
+}
+
+// Result of one face: HLL flux (riemann.py:41-105) with the two
+// well-balanced source terms (reconstruction.py:101-106) already folded into
+// the normal-momentum channel as spatial_operator does (solver.py:503-509).
+struct FaceFlux {
+    float fmass;    // mass flux
+    float fnorm_L;  // normal momentum flux minus source_L (used as "left" flux)
+    float fnorm_R;  // normal momentum flux minus source_R (used as "right" flux)
+    float ftan;     // tangential momentum flux
+    uint32_t speed_bits;  // bit pattern of max(|SL|,|SR|) (>= 0, NaN stays NaN)
+};
+
+// primitive() of a reconstructed face state (riemann.py:20-38).
+SWE_HD void face_primitive(float h0, float hu, float hv, const SweConsts& k, float& h, float& u,
+                           float& v, float& c) {
+    h = fmaxf(h0, 0.0f);
+    bool wet = h > k.dry;
+    float safe = fmaxf(h, k.floor_h);
+    u = wet ? hu / safe : 0.0f;
+    v = wet ? hv / safe : 0.0f;
+    c = wet ? sqrtf(k.g * safe) : 0.0f;
+}
+
+SWE_HD uint32_t f2u(float x) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(x);
+#else
+    union { float f; uint32_t u; } t;
+    t.f = x;
+    return t.u;
+#endif
+}
+
+SWE_HD float u2f(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(x);
+#else
+    union { float f; uint32_t u; } t;
+    t.u = x;
+    return t.f;
+#endif
+}
+
+// One face between cell L and cell R: Lp is L's "p" side, Rm is R's "m"
+// side; hL_c, zL_c, hR_c, zR_c are the two cells' depth and bed.
+// normal_y selects the y-direction conventions of riemann.py:60-61, :199-203.
+SWE_HD FaceFlux face_flux(const Side& Lp, float hL_c, float zL_c, const Side& Rm, float hR_c,
+                          float zR_c, bool normal_y, const SweConsts& k) {
+    // reconstruction.py:59-69
+    float baud = fmaxf(Lp.bed, Rm.bed);
+    float bcn = fminf(baud, fminf(Lp.eta, Rm.eta));
+    float hcL = fmaxf(fminf(Lp.eta - bcn, Lp.hlin), 0.0f);
+    float hcR = fmaxf(fminf(Rm.eta - bcn, Rm.hlin), 0.0f);
+    // reconstruction.py:98-106
+    float UL1 = hcL * Lp.u, UL2 = hcL * Lp.v;
+    float UR1 = hcR * Rm.u, UR2 = hcR * Rm.v;
+    float srcL = (k.half_g * (hL_c + hcL)) * (zL_c - bcn);
+    float srcR = (k.half_g * (hcR + hR_c)) * (zR_c - bcn);
+    // riemann.py:57-105
+    float hL, uL, vL, cL, hR, uR, vR, cR;
+    face_primitive(hcL, UL1, UL2, k, hL, uL, vL, cL);
+    face_primitive(hcR, UR1, UR2, k, hR, uR, vR, cR);
+    float unL = normal_y ? vL : uL, utL = normal_y ? uL : vL;
+    float unR = normal_y ? vR : uR, utR = normal_y ? uR : vR;
+    float us = (0.5f * (unL + unR) + cL) - cR;
+    float cs = 0.5f * (cL + cR) + 0.25f * (unL - unR);
+    float SLw = fminf(unL - cL, us - cs);
+    float SRw = fmaxf(unR + cR, us + cs);
+    bool ldry = hL <= k.dry, rdry = hR <= k.dry;
+    float SL = ldry ? unR - 2.0f * cR : SLw;
+    float SR = rdry ? unL + 2.0f * cL : SRw;
+    float fhL = hL * unL, fhR = hR * unR;
+    float fqL = hL * (unL * unL + k.half_g * hL);
+    float fqR = hR * (unR * unR + k.half_g * hR);
+    float den = fmaxf(SR - SL, k.den_floor);
+    float SLSR = SL * SR;
+    float fhs = ((SR * fhL - SL * fhR) + SLSR * (hR - hL)) / den;
+    float fqs = ((SR * fqL - SL * fqR) + SLSR * (hR * unR - hL * unL)) / den;
+    bool lf = SL >= 0.0f, rf = SR <= 0.0f;
+    float fh = lf ? fhL : (rf ? fhR : fhs);
+    float fq = lf ? fqL : (rf ? fqR : fqs);
+    float ft = (fh > 0.0f ? utL : utR) * fh;
+    bool both = ldry && rdry;
+    FaceFlux F;
+    F.fmass = both ? 0.0f : fh;
+    float fqz = both ? 0.0f : fq;
+    F.ftan = both ? 0.0f : ft;
+    // solver.py:504-509: Fx_left = F - sL, Fx_right = F - sR on the normal channel.
+    F.fnorm_L = fqz - srcL;
+    F.fnorm_R = fqz - srcR;
+    uint32_t a = f2u(SL) & 0x7fffffffu, b = f2u(SR) & 0x7fffffffu;
+    F.speed_bits = both ? 0u : (a > b ? a : b);
+    return F;
+}
+
+// One cell's tendency (solver.py:511-525) from its four faces.  xm/xp are the
+// faces at x-1/2 and x+1/2, ym/yp at y-1/2 and y+1/2.
+struct Rhs {
+    float r0, r1, r2;
+};
+
+SWE_HD Rhs cell_rhs(const FaceFlux& xm, const FaceFlux& xp, const FaceFlux& ym,
+                    const FaceFlux& yp, const SweConsts& k, float rain, float loss) {
+    Rhs r;
+    // x: (Fx_right[x-1/2] - Fx_left[x+1/2]) / dx; channel order (fh, fq, ft)
+    float x0 = (xm.fmass - xp.fmass) / k.dx;
+    float x1 = (xm.fnorm_R - xp.fnorm_L) / k.dx;
+    float x2 = (xm.ftan - xp.ftan) / k.dx;
+    // y: (Gy_top[y-1/2] - Gy_bottom[y+1/2]) / dy; channel order (fh, ft, fq)
+    float y0 = (ym.fmass - yp.fmass) / k.dy;
+    float y1 = (ym.ftan - yp.ftan) / k.dy;
+    float y2 = (ym.fnorm_R - yp.fnorm_L) / k.dy;
+    r.r0 = ((x0 + y0) + rain) - loss;
+    r.r1 = x1 + y1;
+    r.r2 = x2 + y2;
+    return r;
+}
+
+// _clean_and_limit, solver.py:547-570
+struct State {
+    float h, hu, hv;
+};
+
+SWE_HD State clean_and_limit(const State& o, State c, const SweConsts& k, bool positivity) {
+    if (positivity) {
+        float d0 = c.h - o.h, d1 = c.hu - o.hu, d2 = c.hv - o.hv;
+        float safe = fmaxf(-d0, k.eps);
+        float th = d0 < 0.0f ? fminf(o.h / safe, 1.0f) : 1.0f;
+        c.h = o.h + th * d0;
+        c.hu = o.hu + th * d1;
+        c.hv = o.hv + th * d2;
+    }
+    State r;
+    r.h = fmaxf(c.h, 0.0f);
+    bool wet = r.h > k.dry;
+    r.hu = wet ? c.hu : 0.0f;
+    r.hv = wet ? c.hv : 0.0f;
+    return r;
+}
+
+// x ** (float)(1/3) rounded to float (friction.py:66).  Evaluated in double
+// and rounded once; PyTorch's CPU pow agrees with this value on all but a
+// small fraction of inputs, where it differs by one ulp.
+SWE_HD float pow_third(float x, float third) {
+    return (float)pow((double)x, (double)third);
+}
+
+// Semi-implicit friction factor shared by both friction models
+// (friction.py:12-38 and :89, :122).
+SWE_HD State apply_friction_factor(const State& s, float cf_of_h, float dt, const SweConsts& k,
+                                   float speed, float safe, bool wet) {
+    float fac = 1.0f / (1.0f + ((cf_of_h * speed) * dt) / safe);
+    State r;
+    r.h = s.h;
+    r.hu = wet ? s.hu * fac : 0.0f;
+    r.hv = wet ? s.hv * fac : 0.0f;
+    return r;
+}
+
+// apply_manning_friction, friction.py:102-131 (with :12-38, :62-66).  s.h is
+// clamp(U[:,0], min=0) already applied by the caller or here.
+SWE_HD State manning(State s, float n, float dt, const SweConsts& k) {
+    s.h = fmaxf(s.h, 0.0f);
+    bool wet = s.h > k.dry;
+    float safe = fmaxf(s.h, k.fr_vs);
+    float u = (wet ? s.hu : 0.0f) / safe;
+    float v = (wet ? s.hv : 0.0f) / safe;
+    float sp2 = u * u + v * v;
+    bool moving = wet && (sp2 > 0.0f);
+    float speed = moving ? sqrtf(fmaxf(sp2, k.fr_e2)) : 0.0f;
+    float nn = fmaxf(n, 0.0f);
+    float cf = (k.g981 * (nn * nn)) / pow_third(fmaxf(s.h, k.fr_e), k.third);
+    return apply_friction_factor(s, cf, dt, k, speed, safe, wet);
+}
+
+// apply_roughness_length_friction, friction.py:69-99 (with :41-59).
+SWE_HD State roughness_friction(State s, float z0, float dt, const SweConsts& k) {
+    s.h = fmaxf(s.h, 0.0f);
+    bool wet = s.h > k.dry;
+    float safe = fmaxf(s.h, k.fr_vs);
+    float u = (wet ? s.hu : 0.0f) / safe;
+    float v = (wet ? s.hv : 0.0f) / safe;
+    float sp2 = u * u + v * v;
+    bool moving = wet && (sp2 > 0.0f);
+    float speed = moving ? sqrtf(fmaxf(sp2, k.fr_e2)) : 0.0f;
+    float zz = fmaxf(z0, k.fr_e);
+    float ratio = fmaxf(s.h, k.fr_e) / zz;
+    float shallow = 1.0f / fmaxf(0.46f * ratio, k.fr_e);
+    float rc = fmaxf(ratio, k.fr_e);
+    float lt = 2.5f * (((float)log((double)rc) - 1.0f) + (1.0f / rc) * 1.359f);
+    float deep = 1.0f / fmaxf(lt * lt, k.fr_e);
+    float cf = ratio < 2.71828182845904523536f ? shallow : deep;
+    return apply_friction_factor(s, cf, dt, k, speed, safe, wet);
+}
+
+// stable dt, solver.py:620-626: cfl / clamp(ax/dx + ay/dy, min=eps), where
+// PyTorch evaluates `scalar / tensor` as tensor.reciprocal() * scalar.
+SWE_HD float stable_dt(float ax, float ay, const SweConsts& k) {
+    float den = fmaxf(ax / k.dx + ay / k.dy, k.eps);
+    return (1.0f / den) * k.cfl;
+}
+
+}  // namespace swe

@@ -1,0 +1,392 @@
+// swe_step.cu -- fused FP32 step of the DiffSWE2d finite-volume solver on
+// sm_100a, and its C ABI (include/swe_b200.h).
+//
+// One SWE2D.step (src/solver.py:572-663) is two kernel launches:
+//   stage 1: tendency k1 of the state U (spatial_operator, solver.py:448-531)
+//            and the global maxima of the x/y face wave speeds (solver.py:
+//            527-530), reduced in-kernel with warp max + one atomicMax per
+//            warp into the step's reduction words;
+//   stage 2: every block derives dt from those maxima (solver.py:620-626),
+//            forms the predictor clean(U, U + dt/2 k1) on its tile plus a
+//            two-cell halo, the tendency k2 of the predictor on its tile,
+//            the corrector clean(U, U + dt k2) and the friction update
+//            (solver.py:639-661), and writes U_out.
+// The global reduction between the two stages is why the step is two
+// launches: dt depends on every face of the grid.
+//
+// Each block owns a TX x TY tile.  It stages the tile and a two-cell halo
+// (ghost cells of add_ghost_cells, src/boundary.py:150-413, evaluated on the
+// fly at the domain edge) in shared memory as per-cell primitives, then
+// computes per-cell face-side values in both directions, then the HLL face
+// fluxes, then each cell's tendency.  All arithmetic is FP32 on the CUDA
+// cores (swe_math.cuh) in the reference's operation order.
+#include <cuda_runtime.h>
+
+#include "swe_common.cuh"
+
+namespace swe {
+namespace {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int RX = TX + 4, RY = TY + 4;
+constexpr int NXS = TY * (TX + 2);  // x-direction side cells per tile
+constexpr int NYS = (TY + 2) * TX;  // y-direction side cells per tile
+constexpr int NXF = TY * (TX + 1);  // x faces per tile
+constexpr int NYF = (TY + 1) * TX;  // y faces per tile
+
+struct StepArgs {
+    const float* U;
+    const float* bed;
+    const float* n;
+    const float* level;
+    const float* rain;
+    const float* infil;
+    float* tend;   // stage 1: k1 output; stage 2: k1 input
+    float* U_out;  // stage 2 output
+    uint32_t* red;
+    float max_dt, cval;
+    int B, bedB, nB, levelB, ny, nx;
+    int rain_mode, rain_batch, infil_mode, infil_batch;
+    int bc[4];
+    int wsr, positivity, friction, friction_model;
+    SweConsts kc;
+};
+
+__device__ __forceinline__ size_t at3(int b, int c, int j, int i, int ny, int nx) {
+    return (((size_t)b * 3 + c) * ny + j) * nx + i;
+}
+__device__ __forceinline__ size_t at1(int b, int j, int i, int ny, int nx) {
+    return ((size_t)b * ny + j) * nx + i;
+}
+
+__device__ __forceinline__ float forcing(const float* f, int mode, int fb, int b, int j, int i,
+                                         int ny, int nx) {
+    if (mode == SWE_FORCING_SCALAR) return f[0];
+    if (mode == SWE_FORCING_FIELD) return f[at1(fb == 1 ? 0 : b, j, i, ny, nx)];
+    return 0.0f;
+}
+
+// State of interior cell (j, i) as the stage sees it: U for stage 1, the
+// predictor clean(U, U + hdt*k1) (solver.py:639) for stage 2.
+template <int STAGE>
+__device__ __forceinline__ State interior_state(const StepArgs& a, int b, int j, int i, float hdt) {
+    const size_t plane = (size_t)a.ny * a.nx;
+    const size_t o = at3(b, 0, j, i, a.ny, a.nx);
+    State u{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
+    if (STAGE == 1) return u;
+    State c{u.h + hdt * a.tend[o], u.hu + hdt * a.tend[o + plane], u.hv + hdt * a.tend[o + 2 * plane]};
+    return clean_and_limit(u, c, a.kc, a.positivity != 0);
+}
+
+__device__ __forceinline__ float bed_at(const StepArgs& a, int b, int j, int i) {
+    return a.bed[at1(a.bedB == 1 ? 0 : b, j, i, a.ny, a.nx)];
+}
+
+// Padded cell (j, i) (interior coordinates, -2 <= j < ny+2) with the ghost
+// rules of add_ghost_cells.  Only the four "arms" of the padding are ever
+// used by the stencil (corner ghosts feed no face of an interior row or
+// column), so a cell outside the interior in both directions, or beyond the
+// two-cell padding, gets its clamped neighbour's value and is never read.
+template <int STAGE>
+__device__ __forceinline__ void region_cell(const StepArgs& a, int b, int j, int i, float hdt,
+                                            State& s, float& z) {
+    const int ny = a.ny, nx = a.nx;
+    const bool jin = (unsigned)j < (unsigned)ny, iin = (unsigned)i < (unsigned)nx;
+    const int jc = min(max(j, 0), ny - 1), ic = min(max(i, 0), nx - 1);
+    if (jin && iin) {
+        s = interior_state<STAGE>(a, b, j, i, hdt);
+        z = bed_at(a, b, j, i);
+        return;
+    }
+    const bool xarm = jin && i >= -2 && i < nx + 2;
+    const bool yarm = iin && j >= -2 && j < ny + 2;
+    if (!xarm && !yarm) {
+        s = interior_state<STAGE>(a, b, jc, ic, hdt);
+        z = bed_at(a, b, jc, ic);
+        return;
+    }
+    int side, jm, im, jp, ip;
+    if (xarm) {
+        side = i < 0 ? 0 : 1;
+        jm = j;
+        im = i < 0 ? -1 - i : 2 * nx - 1 - i;  // flip of the first/last two columns
+        jp = j;
+        ip = i < 0 ? nx + i : i - nx;
+    } else {
+        side = j < 0 ? 2 : 3;
+        im = i;
+        jm = j < 0 ? -1 - j : 2 * ny - 1 - j;
+        ip = i;
+        jp = j < 0 ? ny + j : j - ny;
+    }
+    const int code = a.bc[side];
+    if (code == SWE_BC_PERIODIC) {  // boundary.py:247-257, :301-302
+        s = interior_state<STAGE>(a, b, jp, ip, hdt);
+        z = bed_at(a, b, jp, ip);
+        return;
+    }
+    z = bed_at(a, b, jc, ic);  // replicate padding of the bed, boundary.py:234-238
+    if (code == SWE_BC_CONSTANT) {  // boundary.py:304-305
+        s = State{a.cval, a.cval, a.cval};
+        return;
+    }
+    s = interior_state<STAGE>(a, b, jc, ic, hdt);  // replicate padding, boundary.py:228-232
+    const float lev = a.level[a.levelB == 1 ? 0 : b];
+    if (code == SWE_BC_WATER_LEVEL) {  // boundary.py:279-282, :307-310
+        s.h = fmaxf(lev - z, 0.0f);
+    } else if (code == SWE_BC_WALL) {  // boundary.py:312-316
+        State m = (jm == jc && im == ic) ? s : interior_state<STAGE>(a, b, jm, im, hdt);
+        if (xarm) s.hu = -m.hu;
+        else s.hv = -m.hv;
+    } else if (code == SWE_BC_ABSORBING) {  // boundary.py:318-328
+        const float hr = fmaxf(lev - z, 0.0f);
+        const float hg = s.h;
+        const float hc = hr > a.kc.absorb_lim ? hr : hg;
+        const float c = sqrtf(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
+        const float cc = (side == 0 || side == 2) ? -c : c;
+        const float val = cc * (hg - hr);
+        if (xarm) s.hu = val;
+        else s.hv = val;
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_max_u32(uint32_t v) { return __reduce_max_sync(0xffffffffu, v); }
+
+template <int STAGE>
+__global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
+    __shared__ float s_h[RY][RX], s_u[RY][RX], s_v[RY][RX], s_eta[RY][RX], s_z[RY][RX];
+    __shared__ Side s_xp[TY][TX + 2], s_xm[TY][TX + 2];
+    __shared__ Side s_yp[TY + 2][TX], s_ym[TY + 2][TX];
+    __shared__ FaceFlux s_fx[TY][TX + 1], s_fy[TY + 1][TX];
+
+    const SweConsts& kc = a.kc;
+    const int tid = threadIdx.x;
+    const int b = blockIdx.z;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+
+    float dt = 0.0f, hdt = 0.0f;
+    if (STAGE == 2) {
+        // solver.py:620-626; torch.minimum propagates a NaN stable dt.
+        const float st = stable_dt(u2f(a.red[0]), u2f(a.red[1]), kc);
+        dt = st != st ? st : fminf(st, a.max_dt);
+        hdt = 0.5f * dt;
+        if (tid == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+            uint32_t st_bits = 0;
+            if (!isfinite(dt)) st_bits |= SWE_S_NONFINITE_DT;
+            else if (!(dt > 0.0f)) st_bits |= SWE_S_NONPOSITIVE_DT;
+            if (st_bits) atomicOr(&a.red[2], st_bits);
+            a.red[3] = f2u(dt);
+        }
+    }
+
+    // Phase 0: primitives of the tile and its two-cell halo.
+    bool bad = false;
+    for (int r = tid; r < RY * RX; r += NT) {
+        const int ry = r / RX, rx = r - ry * RX;
+        const int j = j0 + ry - 2, i = i0 + rx - 2;
+        State s;
+        float z;
+        region_cell<STAGE>(a, b, j, i, hdt, s, z);
+        if (STAGE == 1 && (unsigned)j < (unsigned)a.ny && (unsigned)i < (unsigned)a.nx)
+            bad |= !(isfinite(s.h) && isfinite(s.hu) && isfinite(s.hv));
+        const Prim p = make_prim(s.h, s.hu, s.hv, z, kc);
+        s_h[ry][rx] = p.h;
+        s_u[ry][rx] = p.u;
+        s_v[ry][rx] = p.v;
+        s_eta[ry][rx] = p.eta;
+        s_z[ry][rx] = p.z;
+    }
+    if (STAGE == 1 && __any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(&a.red[2], SWE_S_NONFINITE_STATE);
+    __syncthreads();
+
+    // Phase 1: face-side values (reconstruction.py:26-96) in x and y.
+    const bool wsr = a.wsr != 0;
+    for (int w = tid; w < NXS + NYS; w += NT) {
+        if (w < NXS) {
+            const int ty = w / (TX + 2), sx = w - ty * (TX + 2);
+            const int ry = ty + 2, cx = sx + 1;
+            const Prim pa{s_h[ry][cx - 1], s_u[ry][cx - 1], s_v[ry][cx - 1], s_eta[ry][cx - 1], s_z[ry][cx - 1]};
+            const Prim pc{s_h[ry][cx], s_u[ry][cx], s_v[ry][cx], s_eta[ry][cx], s_z[ry][cx]};
+            const Prim pb{s_h[ry][cx + 1], s_u[ry][cx + 1], s_v[ry][cx + 1], s_eta[ry][cx + 1], s_z[ry][cx + 1]};
+            const Sides sd = make_sides(pa, pc, pb, kc, wsr);
+            s_xp[ty][sx] = sd.p;
+            s_xm[ty][sx] = sd.m;
+        } else {
+            const int w2 = w - NXS;
+            const int sy = w2 / TX, tx = w2 - sy * TX;
+            const int cy = sy + 1, rx = tx + 2;
+            const Prim pa{s_h[cy - 1][rx], s_u[cy - 1][rx], s_v[cy - 1][rx], s_eta[cy - 1][rx], s_z[cy - 1][rx]};
+            const Prim pc{s_h[cy][rx], s_u[cy][rx], s_v[cy][rx], s_eta[cy][rx], s_z[cy][rx]};
+            const Prim pb{s_h[cy + 1][rx], s_u[cy + 1][rx], s_v[cy + 1][rx], s_eta[cy + 1][rx], s_z[cy + 1][rx]};
+            const Sides sd = make_sides(pa, pc, pb, kc, wsr);
+            s_yp[sy][tx] = sd.p;
+            s_ym[sy][tx] = sd.m;
+        }
+    }
+    __syncthreads();
+
+    // Phase 2: HLL fluxes of the faces of the tile (riemann.py:41-105).
+    uint32_t axb = 0u, ayb = 0u;
+    for (int w = tid; w < NXF + NYF; w += NT) {
+        if (w < NXF) {
+            const int ty = w / (TX + 1), fx = w - ty * (TX + 1);
+            const int ry = ty + 2;
+            const FaceFlux F = face_flux(s_xp[ty][fx], s_h[ry][fx + 1], s_z[ry][fx + 1], s_xm[ty][fx + 1],
+                                         s_h[ry][fx + 2], s_z[ry][fx + 2], false, kc);
+            s_fx[ty][fx] = F;
+            if (STAGE == 1 && j0 + ty < a.ny && i0 + fx <= a.nx) axb = max(axb, F.speed_bits);
+        } else {
+            const int w2 = w - NXF;
+            const int fy = w2 / TX, tx = w2 - fy * TX;
+            const int rx = tx + 2;
+            const FaceFlux F = face_flux(s_yp[fy][tx], s_h[fy + 1][rx], s_z[fy + 1][rx], s_ym[fy + 1][tx],
+                                         s_h[fy + 2][rx], s_z[fy + 2][rx], true, kc);
+            s_fy[fy][tx] = F;
+            if (STAGE == 1 && j0 + fy <= a.ny && i0 + tx < a.nx) ayb = max(ayb, F.speed_bits);
+        }
+    }
+    if (STAGE == 1) {
+        axb = warp_max_u32(axb);
+        ayb = warp_max_u32(ayb);
+        if ((tid & 31) == 0) {
+            if (axb) atomicMax(&a.red[0], axb);
+            if (ayb) atomicMax(&a.red[1], ayb);
+        }
+    }
+    __syncthreads();
+
+    // Phase 3: tendency of each tile cell (solver.py:511-525), then for stage 2
+    // the corrector, clean-up and friction (solver.py:646-661).
+    const int ty = tid / TX, tx = tid - (tid / TX) * TX;
+    const int j = j0 + ty, i = i0 + tx;
+    if (j >= a.ny || i >= a.nx) return;
+    const float rain = forcing(a.rain, a.rain_mode, a.rain_batch, b, j, i, a.ny, a.nx);
+    const float loss = fmaxf(forcing(a.infil, a.infil_mode, a.infil_batch, b, j, i, a.ny, a.nx), 0.0f);
+    const Rhs r = cell_rhs(s_fx[ty][tx], s_fx[ty][tx + 1], s_fy[ty][tx], s_fy[ty + 1][tx], kc, rain, loss);
+    const size_t plane = (size_t)a.ny * a.nx;
+    const size_t o = at3(b, 0, j, i, a.ny, a.nx);
+    if (STAGE == 1) {
+        a.tend[o] = r.r0;
+        a.tend[o + plane] = r.r1;
+        a.tend[o + 2 * plane] = r.r2;
+    } else {
+        const State u{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
+        const State c{u.h + dt * r.r0, u.hu + dt * r.r1, u.hv + dt * r.r2};
+        State upd = clean_and_limit(u, c, kc, a.positivity != 0);
+        if (a.friction) {
+            const float nv = a.n[at1(a.nB == 1 ? 0 : b, j, i, a.ny, a.nx)];
+            upd = a.friction_model == 0 ? manning(upd, nv, dt, kc) : roughness_friction(upd, nv, dt, kc);
+        }
+        a.U_out[o] = upd.h;
+        a.U_out[o + plane] = upd.hu;
+        a.U_out[o + 2 * plane] = upd.hv;
+    }
+}
+
+bool fill_common(StepArgs& a, const float* U, const float* bed, int B, int bedB, int ny, int nx,
+                 const swe_params* p, const float* level, int levelB) {
+    if (!U || !bed || !level || !valid_params(p)) return false;
+    if (B < 1 || ny < 2 || nx < 2) return false;  // boundary.py:98-102 (ng = 2)
+    if (bedB != 1 && bedB != B) return false;
+    if (levelB != 1 && levelB != B) return false;
+    if ((long long)ny * nx * 3 * B >= (1ll << 40)) return false;
+    if ((ny + TY - 1) / TY > 65535 || B > 65535) return false;
+    a.U = U;
+    a.bed = bed;
+    a.level = level;
+    a.B = B;
+    a.bedB = bedB;
+    a.levelB = levelB;
+    a.ny = ny;
+    a.nx = nx;
+    a.bc[0] = p->bc_left;
+    a.bc[1] = p->bc_right;
+    a.bc[2] = p->bc_top;
+    a.bc[3] = p->bc_bottom;
+    a.cval = (float)p->constant_value;
+    a.wsr = p->water_slope_reset;
+    a.positivity = p->positivity_limiter;
+    a.friction = p->apply_friction;
+    a.friction_model = p->friction_model;
+    a.kc = make_consts(*p);
+    return true;
+}
+
+bool valid_forcing(const float* f, int mode, int fb, int B) {
+    if (mode == SWE_FORCING_NONE) return true;
+    if (!f) return false;
+    if (mode == SWE_FORCING_SCALAR) return true;
+    if (mode == SWE_FORCING_FIELD) return fb == 1 || fb == B;
+    return false;
+}
+
+dim3 grid_of(const StepArgs& a) { return dim3((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, a.B); }
+
+}  // namespace
+}  // namespace swe
+
+using namespace swe;
+
+extern "C" int swe_spatial_operator_f32(const float* U, const float* bed, int B, int bedB, int ny,
+                                        int nx, const swe_params* p, const float* level, int levelB,
+                                        const float* rain, int rain_mode, int rain_batch,
+                                        const float* infil, int infil_mode, int infil_batch,
+                                        float* rhs, uint32_t* red, void* stream) {
+    StepArgs a{};
+    if (!fill_common(a, U, bed, B, bedB, ny, nx, p, level, levelB) || !rhs || !red) return SWE_EARG;
+    if (!valid_forcing(rain, rain_mode, rain_batch, B) || !valid_forcing(infil, infil_mode, infil_batch, B))
+        return SWE_EARG;
+    a.rain = rain;
+    a.rain_mode = rain_mode;
+    a.rain_batch = rain_batch;
+    a.infil = infil;
+    a.infil_mode = infil_mode;
+    a.infil_batch = infil_batch;
+    a.tend = rhs;
+    a.red = red;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
+    stage_kernel<1><<<grid_of(a), NT, 0, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB,
+                                  const float* n, int nB, int B, int ny, int nx,
+                                  const swe_params* p, const float* level, int levelB,
+                                  float max_dt, const float* infil, int infil_mode,
+                                  int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                                  void* stream) {
+    StepArgs a{};
+    if (stage != 1 && stage != 2 && stage != 3) return SWE_EARG;
+    if (!fill_common(a, U, bed, B, bedB, ny, nx, p, level, levelB)) return SWE_EARG;
+    if (!scratch_k || !red || !U_out || (p->apply_friction && !n)) return SWE_EARG;
+    if (p->apply_friction && nB != 1 && nB != B) return SWE_EARG;
+    if (!valid_forcing(infil, infil_mode, infil_batch, B)) return SWE_EARG;
+    a.n = n;
+    a.nB = nB;
+    a.infil = infil;
+    a.infil_mode = infil_mode;
+    a.infil_batch = infil_batch;
+    a.rain_mode = SWE_FORCING_NONE;
+    a.tend = scratch_k;
+    a.U_out = U_out;
+    a.red = red;
+    a.max_dt = max_dt;
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 g = grid_of(a);
+    if (stage & 1) {
+        if (cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
+        stage_kernel<1><<<g, NT, 0, s>>>(a);
+    }
+    if (stage & 2) stage_kernel<2><<<g, NT, 0, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_step_f32(const float* U, const float* bed, int bedB, const float* n, int nB,
+                            int B, int ny, int nx, const swe_params* p, const float* level,
+                            int levelB, float max_dt, const float* infil, int infil_mode,
+                            int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                            void* stream) {
+    return swe_step_stage_f32(3, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt, infil,
+                              infil_mode, infil_batch, scratch_k, red, U_out, stream);
+}

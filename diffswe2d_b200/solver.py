@@ -1,0 +1,347 @@
+"""SWE2D: the reference's solver module with its step on the B200 kernels.
+
+Drop-in for ``SWE2D`` of ``src/solver.py`` (DiffSWE2d) on the forward path:
+same constructor, buffers and parameter, same ``spatial_operator`` /
+``stable_dt`` / ``step`` / ``forward`` signatures, return types and
+exceptions.  ``step`` runs as the two fused sm_100a kernels of
+``csrc/swe_step.cu``; the host reads one 8-byte word pair per step (status
+and dt), where the reference synchronises three times.
+"""
+from __future__ import annotations
+
+from numbers import Integral, Real
+from typing import Optional, Union
+
+import torch
+import torch.nn as nn
+
+from . import _native as nat
+from .config import SWEConfig
+
+ScalarOrTensor = Union[float, int, torch.Tensor]
+
+
+class SWE2D(nn.Module):
+    """Differentiable B-Flood-style 2-D shallow-water solver (state [h, hu, hv]).
+
+    ``forward(..., t_end=...)`` interprets ``t_end`` as the duration of that
+    call, as the reference does (``src/solver.py:40-47``).
+    """
+
+    def __init__(self, bed_reference, roughness_length, dx, dy, config=None, train_dem=True,
+                 maximum_dem_correction=None, valid_mask=None, x=None, y=None, rainfall=None):
+        super().__init__()
+        self.cfg = config or SWEConfig()
+        self.dx, self.dy = float(dx), float(dy)
+        if self.dx <= 0.0 or self.dy <= 0.0:
+            raise ValueError(f"dx and dy must be positive, got {self.dx}, {self.dy}.")
+        if bed_reference.ndim == 2:
+            bed_reference = bed_reference[None, None]
+        if roughness_length.ndim == 2:
+            roughness_length = roughness_length[None, None]
+        if bed_reference.ndim != 4 or bed_reference.shape[1] != 1:
+            raise ValueError(f"bed_reference must have shape [ny,nx] or [B,1,ny,nx], "
+                             f"got {tuple(bed_reference.shape)}.")
+        if roughness_length.ndim != 4:
+            raise ValueError(f"roughness_length must be 2-D or 4-D, "
+                             f"got {tuple(roughness_length.shape)}.")
+        if bed_reference.shape != roughness_length.shape:
+            raise ValueError(f"DEM and roughness shapes differ: {bed_reference.shape} "
+                             f"!= {roughness_length.shape}.")
+        if not torch.isfinite(bed_reference).all():
+            raise ValueError("bed_reference contains non-finite values.")
+        if not torch.isfinite(roughness_length).all():
+            raise ValueError("roughness_length contains non-finite values.")
+        self.register_buffer("bed_reference", bed_reference.clone())
+        self.register_buffer("roughness_length", roughness_length.clone())
+        mask = (torch.ones_like(bed_reference, dtype=torch.bool) if valid_mask is None
+                else valid_mask.reshape_as(bed_reference).bool())
+        self.register_buffer("valid_mask", mask)
+        if x is not None:
+            self.register_buffer("x", x.clone())
+        if y is not None:
+            self.register_buffer("y", y.clone())
+        self.maximum_dem_correction = maximum_dem_correction
+        self.dem_correction_parameter = nn.Parameter(torch.zeros_like(bed_reference),
+                                                     requires_grad=bool(train_dem))
+        self.train_dem = bool(train_dem)
+        self.rainfall = rainfall
+        self.use_dynamic_bc = False
+        self.bc_times = None
+        self.bc_wls = None
+        self.track_gauges = False
+        self.gauge_indices = {}
+        self.bed_elevations = {}
+        self.ts_time, self.ts_dt = [], []
+        self.ts_h, self.ts_z = {}, {}
+
+    # ------------------------------------------------------------- properties
+    @property
+    def bed(self):
+        """Current bed: bed_reference + correction * mask (src/solver.py:134-147)."""
+        correction = self.dem_correction_parameter
+        if self.maximum_dem_correction is not None:
+            correction = float(self.maximum_dem_correction) * torch.tanh(correction)
+        return self.bed_reference + correction * self.valid_mask.to(self.bed_reference.dtype)
+
+    # ------------------------------------------------------ configuration
+    def set_dynamic_boundary(self, times: torch.Tensor, water_levels: torch.Tensor,
+                             enabled: bool = True) -> None:
+        """Time-varying boundary level (src/solver.py:329-354)."""
+        if not torch.is_tensor(times) or not torch.is_tensor(water_levels):
+            raise TypeError("times and water_levels must be tensors.")
+        if times.ndim != 1 or water_levels.ndim != 1:
+            raise ValueError("times and water_levels must be one-dimensional.")
+        if times.numel() == 0 or times.numel() != water_levels.numel():
+            raise ValueError("Boundary arrays must be non-empty and equal length.")
+        if times.numel() > 1 and not torch.all(times[1:] > times[:-1]):
+            raise ValueError("Dynamic boundary times must be strictly increasing.")
+        if not torch.isfinite(times).all() or not torch.isfinite(water_levels).all():
+            raise ValueError("Dynamic boundary arrays contain non-finite values.")
+        self.bc_times, self.bc_wls = times, water_levels
+        self.use_dynamic_bc = bool(enabled)
+
+    def clear_dynamic_boundary(self) -> None:
+        self.use_dynamic_bc = False
+        self.bc_times = self.bc_wls = None
+
+    def reset_gauge_tracking(self) -> None:
+        self.ts_time, self.ts_dt = [], []
+        self.ts_h = {name: [] for name in self.gauge_indices}
+        self.ts_z = {name: [] for name in self.gauge_indices}
+
+    @staticmethod
+    def _expand(field: torch.Tensor, batch: int) -> torch.Tensor:
+        if field.shape[0] == batch:
+            return field
+        if field.shape[0] != 1:
+            raise ValueError(f"Field batch must be 1 or {batch}, got {field.shape[0]}.")
+        return field.expand(batch, -1, -1, -1)
+
+    @staticmethod
+    def _prepare_boundary_level(level: ScalarOrTensor, reference: torch.Tensor) -> torch.Tensor:
+        if torch.is_tensor(level):
+            return level.to(dtype=reference.dtype, device=reference.device)
+        return reference.new_tensor(level)
+
+    def _interpolate_dynamic_boundary(self, current_time: float,
+                                      reference: torch.Tensor) -> torch.Tensor:
+        """Linear interpolation of the boundary series (src/solver.py:391-415)."""
+        if self.bc_times is None or self.bc_wls is None:
+            raise RuntimeError("Dynamic boundary forcing is not configured.")
+        times = self.bc_times.to(dtype=reference.dtype, device=reference.device)
+        levels = self.bc_wls.to(dtype=reference.dtype, device=reference.device)
+        time = reference.new_tensor(current_time)
+        index = torch.searchsorted(times, time, right=False)
+        index = torch.clamp(index, 1, times.numel() - 1)
+        t0, t1 = times[index - 1], times[index]
+        w0, w1 = levels[index - 1], levels[index]
+        weight = (time - t0) / torch.clamp(t1 - t0, min=torch.finfo(times.dtype).eps)
+        return w0 + weight * (w1 - w0)
+
+    def _resolve_boundary_level(self, current_time: float, U: torch.Tensor,
+                                explicit_boundary_level: Optional[ScalarOrTensor]) -> torch.Tensor:
+        if explicit_boundary_level is not None:
+            return self._prepare_boundary_level(explicit_boundary_level, U)
+        if self.use_dynamic_bc:
+            return self._interpolate_dynamic_boundary(current_time, U)
+        return self._prepare_boundary_level(self.cfg.constant_level, U)
+
+    # ------------------------------------------------------ argument packing
+    def _params(self):
+        return nat.params(self.cfg, self.dx, self.dy)
+
+    @staticmethod
+    def _level_arg(level: torch.Tensor, batch: int):
+        """Boundary value forms of src/boundary.py:113-147 -> (tensor, count)."""
+        lv = level.detach().reshape(-1) if level.ndim > 0 else level.detach().reshape(1)
+        if lv.numel() == 1:
+            return lv.contiguous(), 1
+        if level.ndim == 1 and lv.numel() == batch:
+            return lv.contiguous(), batch
+        raise ValueError("Boundary values must be a scalar, a one-element tensor, or a tensor "
+                         f"with one value per batch member. Received shape {tuple(level.shape)}.")
+
+    @staticmethod
+    def _forcing_arg(value, h: torch.Tensor):
+        """Rain / infiltration argument -> (tensor or None, mode, batch)."""
+        if value is None:
+            return None, nat.FORCING_NONE, 1
+        t = (value.to(dtype=h.dtype, device=h.device) if torch.is_tensor(value)
+             else h.new_tensor(value))
+        if t.numel() == 1:
+            return t.detach().reshape(1).contiguous(), nat.FORCING_SCALAR, 1
+        B, _, ny, nx = h.shape
+        t = t.detach()
+        while t.ndim < 4:
+            t = t.unsqueeze(0)
+        if t.shape[-2:] != (ny, nx) or t.shape[1] != 1 or t.shape[0] not in (1, B):
+            t = torch.broadcast_to(t, (B, 1, ny, nx))
+        return t.contiguous(), nat.FORCING_FIELD, t.shape[0]
+
+    def _check_state(self, U):
+        if U.ndim != 4 or U.shape[1] != 3:
+            raise ValueError(f"U must have shape [batch,3,ny,nx], got {tuple(U.shape)}.")
+        ny, nx = U.shape[-2:]
+        if self.bed_reference.shape[-2:] != (ny, nx):
+            raise ValueError("U and bed must have identical spatial dimensions. "
+                             f"U has {(ny, nx)}; bed has {tuple(self.bed_reference.shape[-2:])}.")
+        if ny < 2 or nx < 2:
+            raise ValueError(f"ng cannot exceed either interior grid dimension. "
+                             f"Received ng=2, ny={ny}, nx={nx}.")
+
+    def _fields(self, U):
+        B = U.shape[0]
+        bed = nat.require_cuda_f32("bed", self.bed.detach())
+        if bed.shape[0] not in (1, B):
+            raise ValueError(f"Field batch must be 1 or {B}, got {bed.shape[0]}.")
+        n = nat.require_cuda_f32("roughness_length", self.roughness_length.detach())
+        if n.shape[0] not in (1, B):
+            raise ValueError(f"Field batch must be 1 or {B}, got {n.shape[0]}.")
+        return bed, n
+
+    # ------------------------------------------------------ spatial operator
+    def spatial_operator(self, U, rainfall_rate=None, infiltration=None, return_wave_speed=False,
+                         boundary_level=None):
+        """Conservative SWE tendency (src/solver.py:448-531)."""
+        self._check_state(U)
+        U = nat.require_cuda_f32("U", U)
+        B, _, ny, nx = U.shape
+        bed, _ = self._fields(U)
+        level = self._prepare_boundary_level(
+            self.cfg.constant_level if boundary_level is None else boundary_level, U)
+        lv, levelB = self._level_arg(level, B)
+        h = U[:, 0:1]
+        rain, rmode, rB = self._forcing_arg(rainfall_rate, h)
+        infil, imode, iB = self._forcing_arg(infiltration, h)
+        rhs = torch.empty_like(U)
+        red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=U.device)
+        p = self._params()
+        rc = nat.lib().swe_spatial_operator_f32(
+            nat.ptr(U), nat.ptr(bed), B, bed.shape[0], ny, nx, p, nat.ptr(lv), levelB,
+            nat.ptr(rain), rmode, rB, nat.ptr(infil), imode, iB, nat.ptr(rhs), nat.ptr(red),
+            nat.stream_handle(U.device))
+        nat.check(rc, "spatial_operator")
+        if return_wave_speed:
+            ax, ay = red[0:2].view(torch.float32).unbind(0)
+            return rhs, ax, ay
+        return rhs
+
+    def stable_dt(self, U, boundary_level=None):
+        """CFL-stable time step (src/solver.py:537-545)."""
+        _, ax, ay = self.spatial_operator(U, return_wave_speed=True, boundary_level=boundary_level)
+        denominator = torch.clamp(ax / self.dx + ay / self.dy, min=self.cfg.epsilon)
+        return self.cfg.cfl / denominator
+
+    # ------------------------------------------------------------------ step
+    def step(self, U, model_time, max_dt, infiltration=None, boundary_level=None):
+        """One adaptive midpoint predictor-corrector step (src/solver.py:572-663).
+
+        Returns ``(U_new, dt_float)``.  The CFL time step is detached, as in
+        the reference.
+        """
+        self._check_state(U)
+        if torch.is_grad_enabled() and (U.requires_grad or (
+                torch.is_tensor(boundary_level) and boundary_level.requires_grad)):
+            from .adjoint import step_with_adjoint
+            return step_with_adjoint(self, U, model_time, max_dt, infiltration, boundary_level)
+        U = nat.require_cuda_f32("U", U)
+        B, _, ny, nx = U.shape
+        max_dt_f = float((max_dt.to(dtype=torch.float32) if torch.is_tensor(max_dt)
+                          else torch.tensor(float(max_dt), dtype=torch.float32)).item())
+        level = self._prepare_boundary_level(
+            self.cfg.constant_level if boundary_level is None else boundary_level, U)
+        U_new, status, dt = self._launch_step(U, level, max_dt_f, infiltration)
+        self._raise_on_status(status, dt)
+        return U_new, dt
+
+    def _launch_step(self, U, level, max_dt_f, infiltration, red=None, scratch=None):
+        """Enqueue one step; returns (U_new, status, dt) with one host read."""
+        B, _, ny, nx = U.shape
+        bed, n = self._fields(U)
+        lv, levelB = self._level_arg(level, B)
+        infil, imode, iB = self._forcing_arg(infiltration, U[:, 0:1])
+        U_out = torch.empty_like(U)
+        scratch = torch.empty_like(U) if scratch is None else scratch
+        red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=U.device) if red is None else red
+        p = self._params()
+        rc = nat.lib().swe_step_f32(
+            nat.ptr(U), nat.ptr(bed), bed.shape[0], nat.ptr(n), n.shape[0], B, ny, nx, p,
+            nat.ptr(lv), levelB, max_dt_f, nat.ptr(infil), imode, iB, nat.ptr(scratch),
+            nat.ptr(red), nat.ptr(U_out), nat.stream_handle(U.device))
+        nat.check(rc, "step")
+        host = red[2:4].cpu()
+        status = int(host[0].item()) & 0xFFFFFFFF
+        dt = float(host[1:2].view(torch.float32).item())
+        return U_out, status, dt
+
+    @staticmethod
+    def _raise_on_status(status: int, dt: float) -> None:
+        if status & (nat.S_NONFINITE_DT | nat.S_NONFINITE_STATE):
+            raise FloatingPointError("The calculated timestep is non-finite.")
+        if status & nat.S_NONPOSITIVE_DT:
+            raise FloatingPointError(f"Non-positive timestep: {dt}.")
+
+    # --------------------------------------------------------------- forward
+    @staticmethod
+    def _scalar_float(value, name: str) -> float:
+        if torch.is_tensor(value):
+            if value.numel() != 1:
+                raise ValueError(f"{name} must be scalar.")
+            return float(value.detach().cpu())
+        if isinstance(value, Real):
+            return float(value)
+        raise TypeError(f"{name} must be a real scalar or scalar tensor.")
+
+    def forward(self, U0, t_end, start_time=0.0, max_steps=1_000_000, infiltration=None,
+                callback=None, boundary_level=None, max_dt_cap=None):
+        """Advance the model for ``t_end`` seconds (src/solver.py:680-779).
+
+        Returns ``(U, hmax)``.
+        """
+        if U0.ndim != 4 or U0.shape[1] != 3:
+            raise ValueError(f"U0 must have shape [batch,3,ny,nx], got {tuple(U0.shape)}.")
+        duration = self._scalar_float(t_end, "t_end")
+        absolute_start = self._scalar_float(start_time, "start_time")
+        if not isinstance(max_steps, Integral) or isinstance(max_steps, bool) or max_steps <= 0:
+            raise ValueError(f"max_steps must be positive, got {max_steps!r}.")
+        if duration < 0.0:
+            raise ValueError(f"t_end duration cannot be negative: {duration}.")
+        if duration == 0.0:
+            return U0, U0[:, 0].clone()
+        U, hmax, elapsed = U0, U0[:, 0].clone(), 0.0
+        tolerance = max(1e-12, 1e-12 * abs(duration))
+        for iteration in range(max_steps):
+            remaining = duration - elapsed
+            if remaining <= tolerance:
+                return U, hmax
+            step_max_dt = remaining
+            if max_dt_cap is not None:
+                step_max_dt = min(remaining, self._scalar_float(max_dt_cap, "max_dt_cap"))
+            current_time = absolute_start + elapsed
+            level = self._resolve_boundary_level(current_time, U, boundary_level)
+            U, dt_value = self.step(U, model_time=current_time, max_dt=step_max_dt,
+                                    infiltration=infiltration, boundary_level=level)
+            hmax = torch.maximum(hmax, U[:, 0])
+            elapsed += dt_value
+            if elapsed > duration and elapsed - duration <= tolerance:
+                elapsed = duration
+            if self.track_gauges:
+                self._record_gauges(U, absolute_start + elapsed, dt_value)
+            if callback is not None:
+                callback(iteration, absolute_start + elapsed, U)
+        raise RuntimeError(f"max_steps={max_steps} reached after {elapsed:.8f} s; "
+                           f"requested duration={duration:.8f} s.")
+
+    def _record_gauges(self, U: torch.Tensor, absolute_time: float, dt_value: float) -> None:
+        """Micro-step gauge records (src/solver.py:781-801)."""
+        self.ts_time.append(absolute_time)
+        self.ts_dt.append(dt_value)
+        current_bed = self.bed
+        for name, (iy, ix) in self.gauge_indices.items():
+            self.ts_h.setdefault(name, [])
+            self.ts_z.setdefault(name, [])
+            depth = float(U[0, 0, iy, ix].detach().cpu())
+            bed = float(current_bed[0, 0, iy, ix].detach().cpu())
+            self.ts_h[name].append(depth)
+            self.ts_z[name].append(depth + bed)

@@ -1,0 +1,114 @@
+/*
+ * swe_b200.h -- C ABI of the B200 shallow-water step library
+ * (diffswe2d_b200/_lib/libswe_b200.so).
+ *
+ * Each entry point replaces one function of the DiffSWE2d reference (cited
+ * as path:line within that project) on the device path.  Conventions:
+ *   - every pointer is a device pointer to contiguous float32 NCHW data
+ *     unless stated otherwise; the caller (PyTorch) allocates every buffer,
+ *     the library keeps no pointer across calls and frees nothing;
+ *   - "B" is the batch, "ny, nx" the interior grid; fields with a batch of 1
+ *     broadcast over the batch (bedB, nB, levelB = 1 or B);
+ *   - work is enqueued on `stream` (a cudaStream_t passed as void*);
+ *     nothing synchronises the host;
+ *   - the return value is SWE_OK or an SWE_E* code; a CUDA launch error is
+ *     reported as SWE_ECUDA.
+ * Numerical failures found on the device (non-finite state or time step,
+ * non-positive time step) are written as SWE_S* bits into a device status
+ * word that the caller reads with the step's time step.
+ */
+#ifndef SWE_B200_H
+#define SWE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. */
+#define SWE_OK 0
+#define SWE_EARG 1  /* invalid argument (shape, size, code) */
+#define SWE_ECUDA 2 /* CUDA launch or runtime error */
+
+/* Device status bits. */
+#define SWE_S_NONFINITE_STATE 1u /* NaN/Inf in the state read by a step */
+#define SWE_S_NONFINITE_DT 2u    /* non-finite CFL time step */
+#define SWE_S_NONPOSITIVE_DT 4u  /* time step <= 0 */
+
+/* Boundary codes (src/boundary.py:11-18). */
+#define SWE_BC_TRANSMISSIVE 0
+#define SWE_BC_PERIODIC 1
+#define SWE_BC_CONSTANT 2
+#define SWE_BC_WATER_LEVEL 3
+#define SWE_BC_WALL 4
+#define SWE_BC_ABSORBING 5
+
+/* Forcing modes for rain / infiltration arguments. */
+#define SWE_FORCING_NONE 0
+#define SWE_FORCING_SCALAR 1 /* one value (device pointer to 1 float) */
+#define SWE_FORCING_FIELD 2  /* [1|B,1,ny,nx]; batch given by *_batch */
+
+/* SWEConfig (src/config.py:4-28) plus grid spacing.  Values are the Python
+ * doubles; the library rounds them to float32 where the reference does. */
+typedef struct swe_params {
+    double gravity, dry_depth, epsilon, cfl, theta, dx, dy;
+    double constant_value;                  /* boundary "constant" */
+    int32_t bc_left, bc_right, bc_top, bc_bottom;
+    int32_t water_slope_reset, positivity_limiter, apply_friction;
+    int32_t friction_model;                 /* 0 manning, 1 roughness length */
+} swe_params;
+
+/* Size in 32-bit words of the reduction/status scratch each step uses:
+ * [0] max x wave speed bits, [1] max y wave speed bits, [2] status bits,
+ * [3] time step (float bits), [4..7] reserved. */
+#define SWE_RED_WORDS 8
+
+/*
+ * SWE2D.spatial_operator(U, rainfall_rate, infiltration,
+ *                        return_wave_speed=True, boundary_level)
+ *   src/solver.py:448-531
+ * rhs [B,3,ny,nx] receives the tendency; red[0], red[1] receive the bit
+ * patterns of the global maxima of the x and y face wave speeds
+ * (solver.py:527-530) and red[2] the status bits.  level holds levelB (1 or
+ * B) water levels for "water_level"/"absorbing" sides.  red is cleared by
+ * the call.
+ */
+int swe_spatial_operator_f32(const float* U, const float* bed, int B, int bedB, int ny, int nx,
+                             const swe_params* p, const float* level, int levelB,
+                             const float* rain, int rain_mode, int rain_batch,
+                             const float* infil, int infil_mode, int infil_batch, float* rhs,
+                             uint32_t* red, void* stream);
+
+/*
+ * SWE2D.step(U, model_time, max_dt, infiltration, boundary_level)
+ *   src/solver.py:572-663 (friction by src/friction.py:69-131)
+ * One adaptive midpoint step: U_out [B,3,ny,nx].  scratch_k is caller-owned
+ * device scratch of B*3*ny*nx floats (the stage-1 tendency); red is
+ * SWE_RED_WORDS words of device scratch, cleared by the call, in which the
+ * step leaves its time step (red[3], float bits) and status (red[2]).
+ * max_dt is the float32 value of the reference's max_dt tensor.
+ */
+int swe_step_f32(const float* U, const float* bed, int bedB, const float* n, int nB, int B,
+                 int ny, int nx, const swe_params* p, const float* level, int levelB,
+                 float max_dt, const float* infil, int infil_mode, int infil_batch,
+                 float* scratch_k, uint32_t* red, float* U_out, void* stream);
+
+/*
+ * The two launches of swe_step_f32, enqueued separately (same arguments):
+ * stage 1 clears red and writes the stage-1 tendency and wave-speed maxima;
+ * stage 2 derives dt and writes U_out; stage 3 is both, i.e. exactly
+ * swe_step_f32.  Callers use the split form to time each kernel with stream
+ * events.  Same reference lines as swe_step_f32.
+ */
+int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB, const float* n,
+                       int nB, int B, int ny, int nx, const swe_params* p, const float* level,
+                       int levelB, float max_dt, const float* infil, int infil_mode,
+                       int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWE_B200_H */

@@ -1,0 +1,302 @@
+"""Generate the golden fixtures of tests/golden/ from the DiffSWE2d reference.
+
+Run in a checkout where the reference source is available (default
+/root/reference); the fixtures it writes are what the tests read, so the
+reference itself never has to be present where the tests run:
+
+    python tests/golden/make_golden.py [--ref /root/reference] [--only ops,c1,c2,adj]
+
+The reference is imported as the package ``diffswe2d`` from its ``src/``
+directory.  Its ``io_netcdf`` module imports ``xarray`` at load time, which
+the step never uses; when xarray is absent a stub module is registered so the
+import succeeds.  All reference runs use PyTorch on the CPU.
+
+Fixtures (numpy .npz, float32 unless noted):
+  ops.npz         operator-level inputs/outputs on small random grids
+  c1_island.npz   256x256 Gaussian-island config, FP32 states at steps
+                  1/10/100/1000 and the FP64 reference (rounded to float32)
+  c2_runup.npz    244x393 runup config with dynamic west water level,
+                  FP32 states at steps 1/50/200 and a forward() chunk
+  adj_small.npz   reference autograd gradients through a short run
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.machinery
+import importlib.util
+import pathlib
+import sys
+import time
+import types
+
+import numpy as np
+import torch
+
+HERE = pathlib.Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+sys.path.insert(0, str(REPO))
+
+from diffswe2d_b200 import scenarios  # noqa: E402
+
+
+def load_reference(root: str):
+    src = pathlib.Path(root) / "src"
+    if "xarray" not in sys.modules:
+        try:
+            import xarray  # noqa: F401
+        except ImportError:
+            stub = types.ModuleType("xarray")
+            stub.__spec__ = importlib.machinery.ModuleSpec("xarray", None)
+            sys.modules["xarray"] = stub
+    spec = importlib.util.spec_from_file_location(
+        "diffswe2d", src / "__init__.py", submodule_search_locations=[str(src)])
+    pkg = importlib.util.module_from_spec(spec)
+    sys.modules["diffswe2d"] = pkg
+    spec.loader.exec_module(pkg)
+    import diffswe2d.boundary as boundary
+    import diffswe2d.friction as friction
+    import diffswe2d.numerics as numerics
+    import diffswe2d.reconstruction as reconstruction
+    import diffswe2d.riemann as riemann
+    return types.SimpleNamespace(pkg=pkg, SWE2D=pkg.SWE2D, SWEConfig=pkg.SWEConfig,
+                                 boundary=boundary, friction=friction, numerics=numerics,
+                                 reconstruction=reconstruction, riemann=riemann)
+
+
+BC_TYPES = ["transmissive", "periodic", "constant", "water_level", "wall", "absorbing"]
+BC_CASES = [
+    ("all_" + t, dict(boundary_left=t, boundary_right=t, boundary_top=t, boundary_bottom=t))
+    for t in BC_TYPES
+] + [
+    ("mixed_a", dict(boundary_left="water_level", boundary_right="wall", boundary_top="periodic",
+                     boundary_bottom="absorbing")),
+    ("mixed_b", dict(boundary_left="constant", boundary_right="transmissive", boundary_top="wall",
+                     boundary_bottom="water_level")),
+    ("mixed_c", dict(boundary_left="periodic", boundary_right="periodic", boundary_top="wall",
+                     boundary_bottom="wall")),
+]
+
+
+def random_state(rng, B, ny, nx, dry_frac=0.25):
+    h = rng.uniform(0.0, 1.0, size=(B, ny, nx))
+    h[rng.uniform(size=h.shape) < dry_frac] = 0.0
+    h[rng.uniform(size=h.shape) < 0.05] = 1e-7  # below dry_depth
+    hu = rng.normal(0.0, 0.3, size=h.shape) * (h > 0)
+    hv = rng.normal(0.0, 0.3, size=h.shape) * (h > 0)
+    U = np.stack([h, hu, hv], axis=1).astype(np.float32)
+    return U
+
+
+def random_bed(rng, B, ny, nx):
+    y, x = np.meshgrid(np.linspace(0, 1, ny), np.linspace(0, 1, nx), indexing="ij")
+    base = -0.5 + 0.8 * x + 0.2 * np.sin(6 * y)
+    bed = base[None, None] + rng.normal(0.0, 0.05, size=(B, 1, ny, nx))
+    return bed.astype(np.float32)
+
+
+def t32(a):
+    return torch.from_numpy(np.ascontiguousarray(a))
+
+
+def make_ops(ref, out):
+    rng = np.random.default_rng(1234)
+    B, ny, nx = 2, 9, 13
+    d = {}
+    U = random_state(rng, B, ny, nx)
+    bed = random_bed(rng, B, ny, nx)
+    bed1 = bed[:1]
+    n = rng.uniform(0.0, 0.05, size=(1, 1, ny, nx)).astype(np.float32)
+    d["U"], d["bed"], d["bed1"], d["n"] = U, bed, bed1, n
+    level_b = np.array([0.15, 0.3], dtype=np.float32)
+    d["level_b"] = level_b
+    cfg0 = ref.SWEConfig()
+    g, eps, dry = cfg0.gravity, cfg0.epsilon, cfg0.dry_depth
+    with torch.no_grad():
+        # primitive / limited increment / minmod
+        h, u, v, c = ref.riemann.primitive(t32(U), g, eps, dry)
+        d["prim_h"], d["prim_u"], d["prim_v"], d["prim_c"] = (x.numpy() for x in (h, u, v, c))
+        q = rng.normal(size=(B, 3, ny, nx)).astype(np.float32)
+        q[:, :, ::3, ::2] = 0.0
+        d["li_q"] = q
+        d["li_x"] = ref.numerics.limited_increment(t32(q), -1, 1.3).numpy()
+        d["li_y"] = ref.numerics.limited_increment(t32(q), -2, 1.3).numpy()
+        # ghost cells for each boundary case, scalar and per-batch level
+        for name, bcs in BC_CASES:
+            for lname, lev in (("s", 0.2), ("b", t32(level_b))):
+                for bname, bb in (("bB", bed), ("b1", bed1)):
+                    Up, zp = ref.boundary.add_ghost_cells(t32(U), t32(bb), 2, constant_value=0.05,
+                                                          constant_level=lev, **bcs)
+                    d[f"gc_{name}_{lname}_{bname}_Up"] = Up.numpy()
+                    d[f"gc_{name}_{lname}_{bname}_zp"] = zp.numpy()
+        # reconstruction + flux on a padded wall grid
+        Up, zp = ref.boundary.add_ghost_cells(t32(U), t32(bed), 2, "wall", "water_level", "wall",
+                                              "transmissive", constant_level=0.2)
+        d["rc_Up"], d["rc_zp"] = Up.numpy(), zp.numpy()
+        for dim, tag in ((-1, "x"), (-2, "y")):
+            for wsr in (True, False):
+                UL, UR, sL, sR = ref.reconstruction.bflood_cn_reconstruction(
+                    Up, zp, dim, g, eps, dry, 1.3, wsr)
+                k = f"rc_{tag}_{int(wsr)}"
+                d[k + "_UL"], d[k + "_UR"], d[k + "_sL"], d[k + "_sR"] = (
+                    x.numpy() for x in (UL, UR, sL, sR))
+            UL, UR, _, _ = ref.reconstruction.bflood_cn_reconstruction(Up, zp, dim, g, eps, dry)
+            F, s = ref.riemann.bflood_hllc_flux(UL, UR, tag, g, eps, dry)
+            d[f"hll_{tag}_UL"], d[f"hll_{tag}_UR"] = UL.numpy(), UR.numpy()
+            d[f"hll_{tag}_F"], d[f"hll_{tag}_s"] = F.numpy(), s.numpy()
+        # friction
+        dt = torch.tensor(0.01, dtype=torch.float32)
+        d["fr_dt"] = np.float32(0.01)
+        d["fr_manning"] = ref.friction.apply_manning_friction(t32(U), t32(n), dt).numpy()
+        z0 = rng.uniform(0.0, 0.02, size=(1, 1, ny, nx)).astype(np.float32)
+        d["fr_z0"] = z0
+        d["fr_rough"] = ref.friction.apply_roughness_length_friction(t32(U), t32(z0), dt).numpy()
+        # spatial operator, clean_and_limit and one/five steps per boundary case
+        for name, bcs in BC_CASES:
+            cfg = ref.SWEConfig(**bcs, constant_value=0.05, constant_level=0.2)
+            m = ref.SWE2D(t32(bed1[0, 0]), t32(n[0, 0]), 0.05, 0.04, config=cfg, train_dem=False)
+            rhs, ax, ay = m.spatial_operator(t32(U), return_wave_speed=True, boundary_level=0.2)
+            d[f"so_{name}_rhs"], d[f"so_{name}_axay"] = rhs.numpy(), np.array([ax, ay], np.float32)
+            Us, dts = t32(U), []
+            for k in range(5):
+                Us, dt_k = m.step(Us, 0.0, 0.05, boundary_level=0.2)
+                dts.append(dt_k)
+                if k == 0:
+                    d[f"st_{name}_1"] = Us.numpy()
+            d[f"st_{name}_5"], d[f"st_{name}_dts"] = Us.numpy(), np.array(dts, np.float64)
+        cand = U + rng.normal(0, 0.2, size=U.shape).astype(np.float32)
+        d["cl_cand"] = cand
+        cfg = ref.SWEConfig()
+        m = ref.SWE2D(t32(bed1[0, 0]), t32(n[0, 0]), 0.05, 0.04, config=cfg, train_dem=False)
+        d["cl_out"] = m._clean_and_limit(t32(U), t32(cand)).numpy()
+        # per-batch bed and level with a batch of two
+        cfg = ref.SWEConfig(boundary_left="water_level", boundary_right="wall",
+                            boundary_top="wall", boundary_bottom="water_level")
+        m = ref.SWE2D(t32(bed), t32(np.broadcast_to(n, bed.shape)), 0.05, 0.04, config=cfg,
+                      train_dem=False)
+        Us, dt_k = m.step(t32(U), 0.0, 0.05, boundary_level=t32(level_b))
+        d["stb_U"], d["stb_dt"] = Us.numpy(), np.float64(dt_k)
+        d["stb_n"] = np.ascontiguousarray(np.broadcast_to(n, bed.shape))
+    np.savez_compressed(out / "ops.npz", **d)
+    print("ops.npz", len(d), "arrays")
+
+
+class correctly_rounded_elementary:
+    """Context manager: evaluate the reference's float32 sqrt and pow correctly
+    rounded (through float64), leaving every other operation untouched.
+
+    PyTorch's CPU build computes float32 sqrt (MKL VML) and pow (SLEEF) to
+    within an ulp but not always correctly rounded; under this patch the
+    reference's step is the exact function that correctly-rounded FP32
+    arithmetic defines, so fixtures made with it pin a correctly-rounded
+    implementation bit for bit.
+    """
+
+    def __enter__(self):
+        self._sqrt, self._pow = torch.sqrt, torch.Tensor.pow
+        sqrt, pow_ = self._sqrt, self._pow
+
+        def cr_sqrt(x, *args, **kwargs):
+            if torch.is_tensor(x) and x.dtype == torch.float32 and not args and not kwargs:
+                return sqrt(x.double()).float()
+            return sqrt(x, *args, **kwargs)
+
+        def cr_pow(self_, exponent):
+            if self_.dtype == torch.float32 and not torch.is_tensor(exponent):
+                return pow_(self_.double(), float(np.float32(exponent))).float()
+            return pow_(self_, exponent)
+
+        torch.sqrt, torch.Tensor.pow = cr_sqrt, cr_pow
+        return self
+
+    def __exit__(self, *exc):
+        torch.sqrt, torch.Tensor.pow = self._sqrt, self._pow
+        return False
+
+
+def run_steps(m, U, nsteps, keep, dyn=None, max_dt=1.0e9):
+    """Drive step() as forward() does for a dynamic boundary, recording states."""
+    states, dts, t = {}, [], 0.0
+    with torch.no_grad():
+        for i in range(1, nsteps + 1):
+            level = None if dyn is None else m._interpolate_dynamic_boundary(t, U)
+            U, dt = m.step(U, t, max_dt, boundary_level=level)
+            t += dt
+            dts.append(dt)
+            if i in keep:
+                states[i] = U.numpy().copy()
+    return states, np.array(dts, np.float64)
+
+
+def make_c1(ref, out):
+    """Gaussian island, 256x256, 1000 steps: stock FP32 and FP64 reference, and
+    the FP32 reference with correctly-rounded sqrt/pow ("f32cr")."""
+    sc = scenarios.gaussian_island(256, seed=0)
+    d = dict(bed=sc.bed, n=sc.roughness, U0=sc.U0, dx=np.float64(sc.dx))
+    keep = (1, 1000)
+    runs = ((torch.float32, "f32", False), (torch.float64, "f64", False), (torch.float32, "f32cr", True))
+    for dtype, tag, cr in runs:
+        cfg = ref.SWEConfig(**sc.config)
+        m = ref.SWE2D(t32(sc.bed).to(dtype), t32(sc.roughness).to(dtype), sc.dx, sc.dy, config=cfg,
+                      train_dem=False)
+        t0 = time.perf_counter()
+        if cr:
+            with correctly_rounded_elementary():
+                states, dts = run_steps(m, t32(sc.U0).to(dtype), 1000, keep)
+        else:
+            states, dts = run_steps(m, t32(sc.U0).to(dtype), 1000, keep)
+        print(f"c1 {tag}: 1000 steps in {time.perf_counter() - t0:.1f}s")
+        for k, v in states.items():
+            if tag != "f32cr" or k == 1000:
+                d[f"{tag}_{k}"] = v.astype(np.float32)
+        d[f"{tag}_dts"] = dts
+    np.savez_compressed(out / "c1_island.npz", **d)
+
+
+def make_c2(ref, out):
+    """Runup, 244x393, dynamic west level: 200 steps (stock and "cr") and a
+    forward() chunk of 0.2 s."""
+    sc = scenarios.runup(seed=0)
+    d = dict(bed=sc.bed, n=sc.roughness, U0=sc.U0, dx=np.float64(sc.dx), bc_times=sc.bc_times,
+             bc_levels=sc.bc_levels)
+    cfg = ref.SWEConfig(**sc.config)
+    m = ref.SWE2D(t32(sc.bed), t32(sc.roughness), sc.dx, sc.dy, config=cfg, train_dem=False)
+    m.set_dynamic_boundary(t32(sc.bc_times), t32(sc.bc_levels))
+    t0 = time.perf_counter()
+    states, dts = run_steps(m, t32(sc.U0), 200, (1, 200), dyn=True)
+    print(f"c2 f32: 200 steps in {time.perf_counter() - t0:.1f}s")
+    for k, v in states.items():
+        d[f"f32_{k}"] = v
+    d["f32_dts"] = dts
+    with correctly_rounded_elementary():
+        cr_states, cr_dts = run_steps(m, t32(sc.U0), 200, (200,), dyn=True)
+        d["f32cr_200"], d["f32cr_dts"] = cr_states[200], cr_dts
+        # forward() chunk of 0.2 s from the 200-step state, starting at 1.0 s
+        count = []
+        with torch.no_grad():
+            U, hmax = m(t32(cr_states[200]), t_end=0.2, start_time=1.0,
+                        callback=lambda it, t, U: count.append(t))
+    d["fwcr_U"], d["fwcr_hmax"], d["fwcr_times"] = U.numpy(), hmax.numpy(), np.array(count, np.float64)
+    np.savez_compressed(out / "c2_runup.npz", **d)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="ops,c1,c2")
+    args = ap.parse_args()
+    torch.set_num_threads(max(1, torch.get_num_threads()))
+    ref = load_reference(args.ref)
+    groups = set(args.only.split(","))
+    if "ops" in groups:
+        make_ops(ref, HERE)
+    if "c1" in groups:
+        make_c1(ref, HERE)
+    if "c2" in groups:
+        make_c2(ref, HERE)
+    if "adj" in groups:
+        from make_golden_adjoint import make_adjoint  # noqa: E402
+        make_adjoint(ref, HERE)
+
+
+if __name__ == "__main__":
+    main()

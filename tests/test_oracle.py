@@ -1,0 +1,123 @@
+"""The CPU oracle against golden outputs of the reference itself.
+
+The oracle (oracle/swe_oracle.c) uses correctly-rounded arithmetic; the
+reference's PyTorch CPU build evaluates sqrt and pow to within an ulp but not
+always correctly rounded.  Operators without sqrt/pow must match bit for bit;
+those with them must agree to a few ulps, and multi-step runs to the
+normwise tolerances written in each test.
+"""
+import numpy as np
+import pytest
+
+from conftest import BC_CASES, bc_kwargs, field_errors, normwise, wet_mask
+from oracle import Oracle, OracleSWE
+
+from diffswe2d_b200.config import SWEConfig
+
+
+@pytest.fixture(scope="module")
+def o32():
+    return Oracle(np.float32)
+
+
+def test_primitive_bit_exact(golden, o32):
+    d = golden("ops")
+    h, u, v, c = o32.primitive(d["U"], SWEConfig())
+    assert np.array_equal(h, d["prim_h"]) and np.array_equal(u, d["prim_u"])
+    assert np.array_equal(v, d["prim_v"]) and np.array_equal(c, d["prim_c"])
+
+
+def test_limited_increment_bit_exact(golden, o32):
+    d = golden("ops")
+    assert np.array_equal(o32.limited_increment(d["li_q"], -1), d["li_x"])
+    assert np.array_equal(o32.limited_increment(d["li_q"], -2), d["li_y"])
+
+
+@pytest.mark.parametrize("case", sorted(BC_CASES))
+@pytest.mark.parametrize("lname", ["s", "b"])
+@pytest.mark.parametrize("bname", ["bB", "b1"])
+def test_ghost_cells_bit_exact(golden, o32, case, lname, bname):
+    d = golden("ops")
+    cfg = SWEConfig(**bc_kwargs(case), constant_value=0.05)
+    bed = d["bed"] if bname == "bB" else d["bed1"]
+    level = 0.2 if lname == "s" else d["level_b"]
+    Up, zp = o32.ghost_cells(d["U"], bed, 2, cfg, level, 0.05)
+    key = f"gc_{case}_{lname}_{bname}"
+    assert np.array_equal(Up, d[key + "_Up"])
+    assert np.array_equal(zp, d[key + "_zp"])
+
+
+@pytest.mark.parametrize("tag,dim", [("x", -1), ("y", -2)])
+@pytest.mark.parametrize("wsr", [1, 0])
+def test_reconstruction_bit_exact(golden, o32, tag, dim, wsr):
+    d = golden("ops")
+    cfg = SWEConfig(water_slope_reset=bool(wsr))
+    UL, UR, sL, sR = o32.reconstruction(d["rc_Up"], d["rc_zp"], dim, cfg)
+    key = f"rc_{tag}_{wsr}"
+    for name, a in (("UL", UL), ("UR", UR), ("sL", sL), ("sR", sR)):
+        assert np.array_equal(a, d[f"{key}_{name}"]), name
+
+
+@pytest.mark.parametrize("tag", ["x", "y"])
+def test_hll_flux_within_sqrt_ulps(golden, o32, tag):
+    d = golden("ops")
+    F, s = o32.hll_flux(d[f"hll_{tag}_UL"], d[f"hll_{tag}_UR"], tag, SWEConfig())
+    # the reference's sqrt can be one ulp off; fluxes inherit a few ulps
+    assert np.allclose(F, d[f"hll_{tag}_F"], rtol=1e-6, atol=1e-7)
+    assert np.allclose(s, d[f"hll_{tag}_s"], rtol=1e-6, atol=0)
+    assert (F != d[f"hll_{tag}_F"]).mean() < 0.02
+
+
+def test_friction(golden, o32):
+    d = golden("ops")
+    assert np.allclose(o32.manning(d["U"], d["n"], d["fr_dt"]), d["fr_manning"], rtol=1e-6, atol=1e-9)
+    assert np.allclose(o32.roughness_friction(d["U"], d["fr_z0"], d["fr_dt"]), d["fr_rough"],
+                       rtol=1e-6, atol=1e-9)
+
+
+def test_clean_and_limit_bit_exact(golden, o32):
+    d = golden("ops")
+    assert np.array_equal(o32.clean_and_limit(d["U"], d["cl_cand"], SWEConfig()), d["cl_out"])
+
+
+@pytest.mark.parametrize("case", sorted(BC_CASES))
+def test_spatial_operator_and_steps(golden, o32, case):
+    d = golden("ops")
+    cfg = SWEConfig(**bc_kwargs(case), constant_value=0.05, constant_level=0.2)
+    rhs, ax, ay = o32.spatial_operator(d["U"], d["bed1"], cfg, 0.05, 0.04, 0.2)
+    assert normwise(rhs, d[f"so_{case}_rhs"]) < 1e-6
+    assert np.allclose([ax, ay], d[f"so_{case}_axay"], rtol=1e-6)
+    m = OracleSWE(d["bed1"], d["n"], 0.05, 0.04, cfg)
+    U = d["U"]
+    dts = []
+    for k in range(5):
+        U, dt = m.step(U, 0.0, 0.05, boundary_level=0.2)
+        dts.append(dt)
+        if k == 0:
+            assert max(field_errors(U, d[f"st_{case}_1"])) < 1e-6
+    assert max(field_errors(U, d[f"st_{case}_5"])) < 1e-5
+    assert np.array_equal(wet_mask(U), wet_mask(d[f"st_{case}_5"]))
+    assert np.allclose(dts, d[f"st_{case}_dts"], rtol=1e-5)
+
+
+def test_batched_bed_and_level(golden):
+    d = golden("ops")
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="water_level")
+    m = OracleSWE(d["bed"], d["stb_n"], 0.05, 0.04, cfg)
+    U, dt = m.step(d["U"], 0.0, 0.05, boundary_level=d["level_b"])
+    assert max(field_errors(U, d["stb_U"])) < 1e-6
+    assert dt == pytest.approx(float(d["stb_dt"]), rel=1e-6)
+
+
+def test_oracle_step_errors():
+    """Non-finite and non-positive dt raise FloatingPointError (src/solver.py:627-632)."""
+    bed = np.full((8, 8), -1.0, np.float32)
+    m = OracleSWE(bed, np.full_like(bed, 0.02), 1.0, 1.0, SWEConfig(boundary_left="wall"))
+    U = np.zeros((1, 3, 8, 8), np.float32)
+    U[:, 0] = 1.0
+    with pytest.raises(FloatingPointError, match="Non-positive"):
+        m.step(U, 0.0, 0.0)
+    U[0, 1, 3, 3] = np.nan
+    with pytest.raises(FloatingPointError, match="non-finite"):
+        m.step(U, 0.0, 1.0)
