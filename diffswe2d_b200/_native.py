@@ -65,6 +65,16 @@ _SIGNATURES = {
                      _P, _I, _I, _P, _P, _P, _P],
     "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                            _F, _P, _I, _I, _P, _P, _P, _P],
+    "swe_ghost_cells_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _I,
+                            _P, _P, _P],
+    "swe_reconstruction_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P, _P,
+                               _P, _P],
+    "swe_hll_flux_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P, _P],
+    "swe_primitive_f32": [_P, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P, _P, _P, _P],
+    "swe_limited_increment_f32": [_P, _I, _I, _I, _I, ctypes.c_double, _P, _P],
+    "swe_minmod3_f32": [_P, _P, _P, ctypes.c_longlong, _P, _P],
+    "swe_clean_and_limit_f32": [_P, _P, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P],
+    "swe_friction_f32": [_P, _P, _I, _I, _I, _I, _F, _I, ctypes.POINTER(SweParams), _P, _P],
 }
 
 _lib = None
@@ -97,9 +107,8 @@ def params(cfg, dx: float, dy: float) -> SweParams:
         if name not in BC_CODES:
             raise ValueError(f"Unsupported {side} boundary type {name!r}. "
                              f"Valid types are {sorted(BC_CODES)}.")
-    if cfg.frictionmodel not in ("manning", "roughness_length") and cfg.apply_friction:
-        # The reference treats every name other than "manning" as roughness length.
-        pass
+    # As in src/solver.py:654-661, every friction model name other than
+    # "manning" selects the roughness-length law.
     return SweParams(
         float(cfg.gravity), float(cfg.dry_depth), float(cfg.epsilon), float(cfg.cfl),
         float(cfg.limiter_theta), float(dx), float(dy), float(cfg.constant_value),
@@ -135,3 +144,13 @@ def check(rc: int, what: str) -> None:
     if rc == SWE_EARG:
         raise ValueError(f"{what}: invalid argument rejected by the CUDA library")
     raise NativeLibraryError(f"{what}: CUDA error (code {rc})")
+
+
+def params_basic(gravity=9.81, epsilon=1e-12, dry_depth=1e-6, theta=1.3,
+                 water_slope_reset=True, positivity_limiter=True, bcs=None,
+                 constant_value=0.0) -> SweParams:
+    """Parameters for the operator-level entry points (no grid spacing)."""
+    l, r, t, b = bcs if bcs is not None else ("transmissive",) * 4
+    return SweParams(float(gravity), float(dry_depth), float(epsilon), 0.5, float(theta), 1.0, 1.0,
+                     float(constant_value), BC_CODES[l], BC_CODES[r], BC_CODES[t], BC_CODES[b],
+                     int(bool(water_slope_reset)), int(bool(positivity_limiter)), 1, 0)

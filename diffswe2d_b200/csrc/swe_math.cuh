@@ -181,25 +181,50 @@ SWE_HD float u2f(uint32_t x) {
 #endif
 }
 
-// One face between cell L and cell R: Lp is L's "p" side, Rm is R's "m"
-// side; hL_c, zL_c, hR_c, zR_c are the two cells' depth and bed.
-// normal_y selects the y-direction conventions of riemann.py:60-61, :199-203.
-SWE_HD FaceFlux face_flux(const Side& Lp, float hL_c, float zL_c, const Side& Rm, float hR_c,
-                          float zR_c, bool normal_y, const SweConsts& k) {
+// Reconstructed states either side of one face and its two well-balanced
+// sources (reconstruction.py:59-106).
+struct FaceStates {
+    float L0, L1, L2;  // UL = (h_cn_L, h_cn_L u_L, h_cn_L v_L)
+    float R0, R1, R2;  // UR
+    float srcL, srcR;  // source_L, source_R
+};
+
+// Lp is L's "p" side, Rm is R's "m" side; hL_c, zL_c, hR_c, zR_c are the two
+// cells' depth and bed.
+SWE_HD FaceStates face_states(const Side& Lp, float hL_c, float zL_c, const Side& Rm, float hR_c,
+                              float zR_c, const SweConsts& k) {
+    FaceStates s;
     // reconstruction.py:59-69
     float baud = fmaxf(Lp.bed, Rm.bed);
     float bcn = fminf(baud, fminf(Lp.eta, Rm.eta));
     float hcL = fmaxf(fminf(Lp.eta - bcn, Lp.hlin), 0.0f);
     float hcR = fmaxf(fminf(Rm.eta - bcn, Rm.hlin), 0.0f);
     // reconstruction.py:98-106
-    float UL1 = hcL * Lp.u, UL2 = hcL * Lp.v;
-    float UR1 = hcR * Rm.u, UR2 = hcR * Rm.v;
-    float srcL = (k.half_g * (hL_c + hcL)) * (zL_c - bcn);
-    float srcR = (k.half_g * (hcR + hR_c)) * (zR_c - bcn);
+    s.L0 = hcL;
+    s.L1 = hcL * Lp.u;
+    s.L2 = hcL * Lp.v;
+    s.R0 = hcR;
+    s.R1 = hcR * Rm.u;
+    s.R2 = hcR * Rm.v;
+    s.srcL = (k.half_g * (hL_c + hcL)) * (zL_c - bcn);
+    s.srcR = (k.half_g * (hcR + hR_c)) * (zR_c - bcn);
+    return s;
+}
+
+// HLL flux of one face (riemann.py:41-105).  Returns the flux in channel
+// order (mass, normal, tangential) via fh/fq/ft (already zeroed where both
+// sides are dry) and the wave speed's bit pattern.
+struct Hll {
+    float fh, fq, ft;
+    uint32_t speed_bits;
+};
+
+SWE_HD Hll hll_flux(float L0, float L1, float L2, float R0, float R1, float R2, bool normal_y,
+                    const SweConsts& k) {
     // riemann.py:57-105
     float hL, uL, vL, cL, hR, uR, vR, cR;
-    face_primitive(hcL, UL1, UL2, k, hL, uL, vL, cL);
-    face_primitive(hcR, UR1, UR2, k, hR, uR, vR, cR);
+    face_primitive(L0, L1, L2, k, hL, uL, vL, cL);
+    face_primitive(R0, R1, R2, k, hR, uR, vR, cR);
     float unL = normal_y ? vL : uL, utL = normal_y ? uL : vL;
     float unR = normal_y ? vR : uR, utR = normal_y ? uR : vR;
     float us = (0.5f * (unL + unR) + cL) - cR;
@@ -221,15 +246,29 @@ SWE_HD FaceFlux face_flux(const Side& Lp, float hL_c, float zL_c, const Side& Rm
     float fq = lf ? fqL : (rf ? fqR : fqs);
     float ft = (fh > 0.0f ? utL : utR) * fh;
     bool both = ldry && rdry;
-    FaceFlux F;
-    F.fmass = both ? 0.0f : fh;
-    float fqz = both ? 0.0f : fq;
-    F.ftan = both ? 0.0f : ft;
-    // solver.py:504-509: Fx_left = F - sL, Fx_right = F - sR on the normal channel.
-    F.fnorm_L = fqz - srcL;
-    F.fnorm_R = fqz - srcR;
+    Hll r;
+    r.fh = both ? 0.0f : fh;
+    r.fq = both ? 0.0f : fq;
+    r.ft = both ? 0.0f : ft;
     uint32_t a = f2u(SL) & 0x7fffffffu, b = f2u(SR) & 0x7fffffffu;
-    F.speed_bits = both ? 0u : (a > b ? a : b);
+    r.speed_bits = both ? 0u : (a > b ? a : b);
+    return r;
+}
+
+// One face between cell L and cell R: reconstruction, HLL flux and the
+// source split of spatial_operator (solver.py:503-509).  normal_y selects
+// the y-direction conventions of riemann.py:60-61, :199-203.
+SWE_HD FaceFlux face_flux(const Side& Lp, float hL_c, float zL_c, const Side& Rm, float hR_c,
+                          float zR_c, bool normal_y, const SweConsts& k) {
+    const FaceStates s = face_states(Lp, hL_c, zL_c, Rm, hR_c, zR_c, k);
+    const Hll h = hll_flux(s.L0, s.L1, s.L2, s.R0, s.R1, s.R2, normal_y, k);
+    FaceFlux F;
+    F.fmass = h.fh;
+    F.ftan = h.ft;
+    // Fx_left = F - sL, Fx_right = F - sR on the normal channel.
+    F.fnorm_L = h.fq - s.srcL;
+    F.fnorm_R = h.fq - s.srcR;
+    F.speed_bits = h.speed_bits;
     return F;
 }
 

@@ -233,6 +233,21 @@ class SWE2D(nn.Module):
         denominator = torch.clamp(ax / self.dx + ay / self.dy, min=self.cfg.epsilon)
         return self.cfg.cfl / denominator
 
+    def _clean_and_limit(self, old, candidate):
+        """Positivity preservation and dry-cell momentum removal (src/solver.py:547-570)."""
+        old = nat.require_cuda_f32("old", old)
+        candidate = nat.require_cuda_f32("candidate", candidate)
+        if old.shape != candidate.shape or old.ndim != 4 or old.shape[1] != 3:
+            raise ValueError(f"old and candidate must both be [B,3,ny,nx], got "
+                             f"{tuple(old.shape)} and {tuple(candidate.shape)}.")
+        B, _, ny, nx = old.shape
+        out = torch.empty_like(old)
+        rc = nat.lib().swe_clean_and_limit_f32(nat.ptr(old), nat.ptr(candidate), B, ny, nx,
+                                               self._params(), nat.ptr(out),
+                                               nat.stream_handle(old.device))
+        nat.check(rc, "_clean_and_limit")
+        return out
+
     # ------------------------------------------------------------------ step
     def step(self, U, model_time, max_dt, infiltration=None, boundary_level=None):
         """One adaptive midpoint predictor-corrector step (src/solver.py:572-663).

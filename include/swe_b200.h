@@ -107,6 +107,69 @@ int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB, co
                        int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                        void* stream);
 
+/* ---------------------------------------------------------------------
+ * Operator-level entry points (the reference's numerical operators).
+ * --------------------------------------------------------------------- */
+
+/*
+ * add_ghost_cells(U, bed, ng, boundary_*, constant_value, constant_level)
+ *   src/boundary.py:150-413
+ * Up [B,3,ny+2ng,nx+2ng] and zp [bedB,1,ny+2ng,nx+2ng], including the
+ * corner cells as the reference's left/right/top/bottom overwrites leave
+ * them.  level and constant_value hold levelB / cvalB (1 or B) values.
+ */
+int swe_ghost_cells_f32(const float* U, const float* bed, int B, int bedB, int ny, int nx, int ng,
+                        const swe_params* p, const float* level, int levelB,
+                        const float* constant_value, int cvalB, float* Up, float* zp,
+                        void* stream);
+
+/*
+ * bflood_cn_reconstruction(U, bed, dim, gravity, epsilon, dry_depth, theta,
+ *                          water_slope_reset)   src/reconstruction.py:18-108
+ * Up [B,3,H,W], zp [zB,1,H,W]; dim = -1 (x) or -2 (y), with torch.roll
+ * wrap-around at the array ends.  UL, UR [B,3,H,W]; sL, sR [B,1,H,W].
+ */
+int swe_reconstruction_f32(const float* Up, const float* zp, int B, int zB, int H, int W, int dim,
+                           const swe_params* p, float* UL, float* UR, float* sL, float* sR,
+                           void* stream);
+
+/*
+ * bflood_hllc_flux(UL, UR, normal, gravity, epsilon, dry_depth)
+ *   src/riemann.py:41-105
+ * UL, UR [B,3,H,W] -> flux [B,3,H,W], speed [B,1,H,W]; normal_y = 0 for
+ * "x", 1 for "y".
+ */
+int swe_hll_flux_f32(const float* UL, const float* UR, int B, int H, int W, int normal_y,
+                     const swe_params* p, float* flux, float* speed, void* stream);
+
+/* primitive(U, gravity, epsilon, dry_depth)   src/riemann.py:20-38
+ * U [B,3,H,W] -> h, u, v, c [B,1,H,W]. */
+int swe_primitive_f32(const float* U, int B, int H, int W, const swe_params* p, float* h,
+                      float* u, float* v, float* c, void* stream);
+
+/* limited_increment(q, dim, theta)   src/numerics.py:16-27
+ * q is `outer` contiguous [H,W] planes; dim = -1 or -2 (roll wrap-around). */
+int swe_limited_increment_f32(const float* q, int outer, int H, int W, int dim, double theta,
+                              float* out, void* stream);
+
+/* minmod3(a, b, c)   src/numerics.py:4-13, elementwise over n values. */
+int swe_minmod3_f32(const float* a, const float* b, const float* c, long long n, float* out,
+                    void* stream);
+
+/* SWE2D._clean_and_limit(old, candidate)   src/solver.py:547-570 */
+int swe_clean_and_limit_f32(const float* old, const float* cand, int B, int ny, int nx,
+                            const swe_params* p, float* out, void* stream);
+
+/*
+ * apply_manning_friction (model 0)      src/friction.py:102-131
+ * apply_roughness_length_friction (1)   src/friction.py:69-99
+ * U [B,3,ny,nx], n (Manning n or roughness length) [nB,1,ny,nx]; dt is
+ * the float32 time step; p->dry_depth and p->epsilon are the functions'
+ * dry_depth / epsilon arguments.
+ */
+int swe_friction_f32(const float* U, const float* n, int nB, int B, int ny, int nx, float dt,
+                     int model, const swe_params* p, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
