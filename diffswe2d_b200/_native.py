@@ -65,6 +65,8 @@ _SIGNATURES = {
                      _P, _I, _I, _P, _P, _P, _P],
     "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                            _F, _P, _I, _I, _P, _P, _P, _P],
+    "swe_step_noalloc_f32": [_P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
+                             _F, _P, _I, _I, _P, _P, _P],
     "swe_ghost_cells_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _I,
                             _P, _P, _P],
     "swe_reconstruction_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P, _P,

@@ -22,6 +22,8 @@
 // cores (swe_math.cuh) in the reference's operation order.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "swe_common.cuh"
 
 namespace swe {
@@ -389,4 +391,64 @@ extern "C" int swe_step_f32(const float* U, const float* bed, int bedB, const fl
                             void* stream) {
     return swe_step_stage_f32(3, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt, infil,
                               infil_mode, infil_batch, scratch_k, red, U_out, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Step without allocation: scratch in a static device array.
+//
+// For callers that cannot allocate device memory (their device memory is
+// owned by another allocator, or they may not allocate after start-up), the
+// stage-1 tendency and the reduction words live in this array instead of
+// caller buffers.  Layout: words [0, 64) reduction/status (SWE_RED_WORDS
+// used, the rest keeps the tendency 256-byte aligned), then 3 planes of
+// SWE_NOALLOC_MAX_CELLS floats for the tendency.  In host code the name
+// g_noalloc_scratch is only a host-side stand-in; the device address is
+// looked up once per device with cudaGetSymbolAddress.
+namespace {
+
+constexpr size_t kNoallocRedWords = 64;
+constexpr size_t kNoallocWords = kNoallocRedWords + 3 * (size_t)SWE_NOALLOC_MAX_CELLS;
+
+static __device__ __align__(256) float g_noalloc_scratch[kNoallocWords];
+
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mutex;
+float* g_noalloc_base[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up on
+// the first call per device, then cached).
+int noalloc_scratch(float** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SWE_ECUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        void* addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return SWE_ECUDA;
+        g_noalloc_base[dev] = static_cast<float*>(addr);
+    }
+    *out = g_noalloc_base[dev];
+    return SWE_OK;
+}
+
+}  // namespace
+
+extern "C" int swe_step_noalloc_f32(const float* U, const float* bed, int bedB, const float* n,
+                                    int nB, int B, int ny, int nx, const swe_params* p,
+                                    const float* level, int levelB, float max_dt,
+                                    const float* infil, int infil_mode, int infil_batch,
+                                    float* U_out, uint32_t* status_dt, void* stream) {
+    if (!status_dt || B < 1 || ny < 1 || nx < 1) return SWE_EARG;
+    if ((long long)B * ny * nx > (long long)SWE_NOALLOC_MAX_CELLS) return SWE_ETOOLARGE;
+    float* base = nullptr;
+    const int rc0 = noalloc_scratch(&base);
+    if (rc0 != SWE_OK) return rc0;
+    uint32_t* red = reinterpret_cast<uint32_t*>(base);
+    float* scratch_k = base + kNoallocRedWords;
+    const int rc = swe_step_stage_f32(3, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt,
+                                      infil, infil_mode, infil_batch, scratch_k, red, U_out, stream);
+    if (rc != SWE_OK) return rc;
+    if (cudaMemcpyAsync(status_dt, red + 2, 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                        (cudaStream_t)stream) != cudaSuccess)
+        return SWE_ECUDA;
+    return SWE_OK;
 }

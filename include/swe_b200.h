@@ -107,6 +107,36 @@ int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB, co
                        int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                        void* stream);
 
+/*
+ * swe_step_noalloc_f32 -- one step like swe_step_f32, for callers that must
+ * not allocate device memory.  No counterpart in the reference: it exists
+ * for hosts whose device memory belongs to another allocator (a framework's
+ * caching allocator or memory pool) or that forbid allocation after
+ * start-up (a real-time control loop), and so cannot hand the step the
+ * scratch_k / red buffers that swe_step_f32 takes.
+ *
+ * The scratch lives in a static device array inside the library, sized for
+ * B*ny*nx <= SWE_NOALLOC_MAX_CELLS cells (12 MiB plus 256 bytes); every GPU
+ * that loads the library holds that array until the process exits.  Larger
+ * grids are rejected with SWE_ETOOLARGE before anything is enqueued.
+ * The call allocates nothing: it issues one memset and the two step kernels
+ * on `stream`, and copies the step's status word and time step (float
+ * bits) into status_dt[0..1] (device memory, provided by the caller).
+ * The first call on a device looks up the array's device address with that
+ * device current (once per device, cached); make that first call before
+ * any stream capture.  All calls share the one array and it keeps the last
+ * call's contents (the call clears the words that must start at zero), so
+ * calls that overlap on the GPU -- on different streams, or from different
+ * host threads without ordering -- race and give wrong results.
+ */
+#define SWE_ETOOLARGE 3 /* grid larger than the static scratch of the no-alloc step */
+#define SWE_NOALLOC_MAX_CELLS (1 << 20)
+
+int swe_step_noalloc_f32(const float* U, const float* bed, int bedB, const float* n, int nB,
+                         int B, int ny, int nx, const swe_params* p, const float* level,
+                         int levelB, float max_dt, const float* infil, int infil_mode,
+                         int infil_batch, float* U_out, uint32_t* status_dt, void* stream);
+
 /* ---------------------------------------------------------------------
  * Operator-level entry points (the reference's numerical operators).
  * --------------------------------------------------------------------- */
