@@ -53,6 +53,27 @@ class SweParams(ctypes.Structure):
     ]
 
 
+class SweClock(ctypes.Structure):
+    """swe_clock of include/swe_b200.h (72 bytes)."""
+    _fields_ = [
+        ("duration", ctypes.c_double),
+        ("start", ctypes.c_double),
+        ("tolerance", ctypes.c_double),
+        ("max_dt_cap", ctypes.c_double),
+        ("elapsed", ctypes.c_double),
+        ("max_steps", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("active", ctypes.c_int32),
+        ("state", ctypes.c_int32),
+        ("dt_status", ctypes.c_uint32),
+        ("max_dt", ctypes.c_float),
+        ("level", ctypes.c_float),
+        ("last_dt", ctypes.c_float),
+    ]
+
+
+CLOCK_RUNNING, CLOCK_DONE, CLOCK_MAXSTEPS, CLOCK_FAILED = 0, 1, 2, 3
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -65,6 +86,9 @@ _SIGNATURES = {
                      _P, _I, _I, _P, _P, _P, _P],
     "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                            _F, _P, _I, _I, _P, _P, _P, _P],
+    "swe_clock_f32": [_P, _P, _P, _P, _I, _P, _P, _I, _I, _P, _I, _P, _I, _P],
+    "swe_step_clocked_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
+                             _P, _P, _I, _I, _P, _P, _P, _P, _P],
     "swe_step_noalloc_f32": [_P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _F, _P, _I, _I, _P, _P, _P],
     "swe_ghost_cells_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _I,
@@ -77,6 +101,7 @@ _SIGNATURES = {
     "swe_minmod3_f32": [_P, _P, _P, ctypes.c_longlong, _P, _P],
     "swe_clean_and_limit_f32": [_P, _P, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P],
     "swe_friction_f32": [_P, _P, _I, _I, _I, _I, _F, _I, ctypes.POINTER(SweParams), _P, _P],
+    "swe_selftest_arith_f32": [_I, ctypes.c_longlong, ctypes.c_ulonglong, _P, _P, _P],
 }
 
 _lib = None

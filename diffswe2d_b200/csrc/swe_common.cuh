@@ -2,12 +2,31 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include "../../include/swe_b200.h"
 #include "swe_math.cuh"
 
 namespace swe {
+
+// RN(1/b) for a finite float b != 0, exactly: the candidate from double
+// division and its two float neighbours are compared by the exact residual
+// |1 - b y| (a product of two floats is exact in double).
+inline float host_rcp_cr(float b) {
+    float y = (float)(1.0 / (double)b);
+    float best = y;
+    double best_err = fabs(1.0 - (double)b * (double)y);
+    for (int d = -1; d <= 1; d += 2) {
+        float c = nextafterf(y, d < 0 ? -INFINITY : INFINITY);
+        double err = fabs(1.0 - (double)b * (double)c);
+        if (err < best_err) {
+            best = c;
+            best_err = err;
+        }
+    }
+    return best;
+}
 
 // Derives the float32 constants of swe_params as the reference rounds its
 // Python scalars (see SweConsts).
@@ -35,7 +54,8 @@ inline SweConsts make_consts(const swe_params& p) {
     k.absorb_lim = 1e-4f;
     k.absorb_min = 1e-6f;
     k.g981 = 9.81f;
-    k.wall_pad0 = k.wall_pad1 = 0.0f;
+    k.rdx = host_rcp_cr(k.dx);
+    k.rdy = host_rcp_cr(k.dy);
     return k;
 }
 

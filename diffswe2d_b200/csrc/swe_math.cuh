@@ -42,8 +42,114 @@ struct SweConsts {
     float absorb_lim; // 1e-4                             boundary.py:325
     float absorb_min; // 1e-6                             boundary.py:326
     float g981;       // 9.81 (hard-coded)                friction.py:66, boundary.py:326
-    float wall_pad0, wall_pad1;  // unused padding, keeps 16-byte multiples
+    float rdx, rdy;   // RN(1/dx), RN(1/dy) for the tendency's divisions
 };
+
+// ------------------------------------------------ correctly rounded division
+// Quotients are IEEE correctly rounded, as the reference's float32 "/"
+// is.  On the device several quotients that share a denominator b share one
+// reciprocal y = RN(1/b): the hardware approximation rcp.approx refined by
+// one Newton-Raphson step y1 = y0 + y0 (1 - b y0), then each quotient is
+// q = RN(a y) corrected once with the exact FMA remainder r = a - q b,
+// q' = RN(q + r y) (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The
+// device self-test swe_selftest_arith_f32 checks rcp_cr against CUDA's
+// rcp.rn for every float in the range used and div_by against div.rn on
+// random and near-halfway operands.  Quotients outside [2^-100, 2^100]
+// (zero excepted) and non-finite operands take the IEEE division instead.
+SWE_HD float rcp_cr(float b) {
+#if defined(__CUDA_ARCH__)
+    float y0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(b));
+    const float e = __fmaf_rn(-b, y0, 1.0f);
+    const float y1 = __fmaf_rn(y0, e, y0);
+    const float ab = fabsf(b);
+    return (ab >= 0x1p-100f && ab < 0x1p+100f) ? y1 : __frcp_rn(b);
+#else
+    return 1.0f / b;
+#endif
+}
+
+// a / b given y = rcp_cr(b).
+SWE_HD float div_by(float a, float b, float y) {
+#if defined(__CUDA_ARCH__)
+    const float q = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-q, b, a);
+    const float q1 = __fmaf_rn(r, y, q);
+    const float aq = fabsf(q);
+    const bool safe = (aq >= 0x1p-100f && aq <= 0x1p+100f) || a == 0.0f;
+    return safe ? q1 : __fdiv_rn(a, b);
+#else
+    (void)y;
+    return a / b;
+#endif
+}
+
+// Correctly rounded square root for finite x > 0: s = x y and h = y/2 from
+// the hardware approximation y ~ 1/sqrt(x) (rsqrt.approx), corrected once
+// with the exact FMA remainder r = x - s s, s' = RN(s + r h) (Markstein's
+// method for the square root, same reference).  Checked exhaustively
+// against sqrt.rn over [2^-100, 2^100) by swe_selftest_arith_f32; other
+// arguments take the IEEE square root.
+SWE_HD float sqrt_cr(float x) {
+#if defined(__CUDA_ARCH__)
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    const float s = __fmul_rn(x, y);
+    const float h = __fmul_rn(0.5f, y);
+    const float r = __fmaf_rn(-s, s, x);
+    const float s1 = __fmaf_rn(r, h, s);
+    const bool safe = x >= 0x1p-100f && x < 0x1p+100f;
+    return safe ? s1 : __fsqrt_rn(x);
+#else
+    return sqrtf(x);
+#endif
+}
+
+// The step's quotients, reciprocals and square roots.  With SWE_FAST_DIV the
+// shared-reciprocal forms above are used, otherwise CUDA's IEEE operations;
+// both give the same correctly-rounded values.
+#ifndef SWE_FAST_DIV
+#define SWE_FAST_DIV 1
+#endif
+
+// Reciprocal of a denominator shared by several quotients (unused when
+// SWE_FAST_DIV is off).
+SWE_HD float shared_rcp(float b) {
+#if SWE_FAST_DIV
+    return rcp_cr(b);
+#else
+    (void)b;
+    return 0.0f;
+#endif
+}
+
+// a / b with y = shared_rcp(b).
+SWE_HD float quot(float a, float b, float y) {
+#if SWE_FAST_DIV
+    return div_by(a, b, y);
+#else
+    (void)y;
+    return a / b;
+#endif
+}
+
+// 1 / b (PyTorch's reciprocal()).
+SWE_HD float recip(float b) {
+#if SWE_FAST_DIV
+    return rcp_cr(b);
+#else
+    return 1.0f / b;
+#endif
+}
+
+SWE_HD float root(float x) {
+#if SWE_FAST_DIV
+    return sqrt_cr(x);
+#else
+    return sqrtf(x);
+#endif
+}
 
 // ---------------------------------------------------------------- numerics
 // minmod3, numerics.py:4-13.  With lo = min(a,b,c) and hi = max(a,b,c):
@@ -75,8 +181,9 @@ SWE_HD Prim make_prim(float U0, float U1, float U2, float z, const SweConsts& k)
     p.h = fmaxf(U0, 0.0f);
     bool wet = p.h > k.dry;
     float safe = fmaxf(p.h, k.floor_h);
-    p.u = wet ? U1 / safe : 0.0f;
-    p.v = wet ? U2 / safe : 0.0f;
+    float y = shared_rcp(safe);
+    p.u = wet ? quot(U1, safe, y) : 0.0f;
+    p.v = wet ? quot(U2, safe, y) : 0.0f;
     p.eta = p.h + z;
     p.z = z;
     return p;
@@ -123,7 +230,7 @@ SWE_HD Sides make_sides(const Prim& a, const Prim& c, const Prim& b, const SweCo
     s.p.bed = c.z + hdz;    // :56
     s.m.bed = c.z - hdz;    // :57
     float safe = fmaxf(c.h, k.floor_h);  // :71-73
-    float q = hdh / safe;                // 0.5 * dh / safe_h, :75-76
+    float q = quot(hdh, safe, shared_rcp(safe));  // 0.5 * dh / safe_h, :75-76
     bool wet = c.h > k.dry;              // :78-87
     float fL = wet ? 1.0f - q : 1.0f;
     float fR = wet ? 1.0f + q : 1.0f;
@@ -156,9 +263,10 @@ SWE_HD void face_primitive(float h0, float hu, float hv, const SweConsts& k, flo
     h = fmaxf(h0, 0.0f);
     bool wet = h > k.dry;
     float safe = fmaxf(h, k.floor_h);
-    u = wet ? hu / safe : 0.0f;
-    v = wet ? hv / safe : 0.0f;
-    c = wet ? sqrtf(k.g * safe) : 0.0f;
+    float y = shared_rcp(safe);
+    u = wet ? quot(hu, safe, y) : 0.0f;
+    v = wet ? quot(hv, safe, y) : 0.0f;
+    c = wet ? root(k.g * safe) : 0.0f;
 }
 
 SWE_HD uint32_t f2u(float x) {
@@ -238,9 +346,10 @@ SWE_HD Hll hll_flux(float L0, float L1, float L2, float R0, float R1, float R2, 
     float fqL = hL * (unL * unL + k.half_g * hL);
     float fqR = hR * (unR * unR + k.half_g * hR);
     float den = fmaxf(SR - SL, k.den_floor);
+    float yden = shared_rcp(den);
     float SLSR = SL * SR;
-    float fhs = ((SR * fhL - SL * fhR) + SLSR * (hR - hL)) / den;
-    float fqs = ((SR * fqL - SL * fqR) + SLSR * (hR * unR - hL * unL)) / den;
+    float fhs = quot((SR * fhL - SL * fhR) + SLSR * (hR - hL), den, yden);
+    float fqs = quot((SR * fqL - SL * fqR) + SLSR * (hR * unR - hL * unL), den, yden);
     bool lf = SL >= 0.0f, rf = SR <= 0.0f;
     float fh = lf ? fhL : (rf ? fhR : fhs);
     float fq = lf ? fqL : (rf ? fqR : fqs);
@@ -282,13 +391,13 @@ SWE_HD Rhs cell_rhs(const FaceFlux& xm, const FaceFlux& xp, const FaceFlux& ym,
                     const FaceFlux& yp, const SweConsts& k, float rain, float loss) {
     Rhs r;
     // x: (Fx_right[x-1/2] - Fx_left[x+1/2]) / dx; channel order (fh, fq, ft)
-    float x0 = (xm.fmass - xp.fmass) / k.dx;
-    float x1 = (xm.fnorm_R - xp.fnorm_L) / k.dx;
-    float x2 = (xm.ftan - xp.ftan) / k.dx;
+    float x0 = quot(xm.fmass - xp.fmass, k.dx, k.rdx);
+    float x1 = quot(xm.fnorm_R - xp.fnorm_L, k.dx, k.rdx);
+    float x2 = quot(xm.ftan - xp.ftan, k.dx, k.rdx);
     // y: (Gy_top[y-1/2] - Gy_bottom[y+1/2]) / dy; channel order (fh, ft, fq)
-    float y0 = (ym.fmass - yp.fmass) / k.dy;
-    float y1 = (ym.ftan - yp.ftan) / k.dy;
-    float y2 = (ym.fnorm_R - yp.fnorm_L) / k.dy;
+    float y0 = quot(ym.fmass - yp.fmass, k.dy, k.rdy);
+    float y1 = quot(ym.ftan - yp.ftan, k.dy, k.rdy);
+    float y2 = quot(ym.fnorm_R - yp.fnorm_L, k.dy, k.rdy);
     r.r0 = ((x0 + y0) + rain) - loss;
     r.r1 = x1 + y1;
     r.r2 = x2 + y2;
@@ -304,7 +413,7 @@ SWE_HD State clean_and_limit(const State& o, State c, const SweConsts& k, bool p
     if (positivity) {
         float d0 = c.h - o.h, d1 = c.hu - o.hu, d2 = c.hv - o.hv;
         float safe = fmaxf(-d0, k.eps);
-        float th = d0 < 0.0f ? fminf(o.h / safe, 1.0f) : 1.0f;
+        float th = d0 < 0.0f ? fminf(quot(o.h, safe, shared_rcp(safe)), 1.0f) : 1.0f;
         c.h = o.h + th * d0;
         c.hu = o.hu + th * d1;
         c.hv = o.hv + th * d2;
@@ -328,7 +437,7 @@ SWE_HD float pow_third(float x, float third) {
 // (friction.py:12-38 and :89, :122).
 SWE_HD State apply_friction_factor(const State& s, float cf_of_h, float dt, const SweConsts& k,
                                    float speed, float safe, bool wet) {
-    float fac = 1.0f / (1.0f + ((cf_of_h * speed) * dt) / safe);
+    float fac = recip(1.0f + quot((cf_of_h * speed) * dt, safe, shared_rcp(safe)));
     State r;
     r.h = s.h;
     r.hu = wet ? s.hu * fac : 0.0f;
@@ -342,13 +451,15 @@ SWE_HD State manning(State s, float n, float dt, const SweConsts& k) {
     s.h = fmaxf(s.h, 0.0f);
     bool wet = s.h > k.dry;
     float safe = fmaxf(s.h, k.fr_vs);
-    float u = (wet ? s.hu : 0.0f) / safe;
-    float v = (wet ? s.hv : 0.0f) / safe;
+    float ys = shared_rcp(safe);
+    float u = quot(wet ? s.hu : 0.0f, safe, ys);
+    float v = quot(wet ? s.hv : 0.0f, safe, ys);
     float sp2 = u * u + v * v;
     bool moving = wet && (sp2 > 0.0f);
-    float speed = moving ? sqrtf(fmaxf(sp2, k.fr_e2)) : 0.0f;
+    float speed = moving ? root(fmaxf(sp2, k.fr_e2)) : 0.0f;
     float nn = fmaxf(n, 0.0f);
-    float cf = (k.g981 * (nn * nn)) / pow_third(fmaxf(s.h, k.fr_e), k.third);
+    float pw = pow_third(fmaxf(s.h, k.fr_e), k.third);
+    float cf = quot(k.g981 * (nn * nn), pw, shared_rcp(pw));
     return apply_friction_factor(s, cf, dt, k, speed, safe, wet);
 }
 
@@ -357,17 +468,18 @@ SWE_HD State roughness_friction(State s, float z0, float dt, const SweConsts& k)
     s.h = fmaxf(s.h, 0.0f);
     bool wet = s.h > k.dry;
     float safe = fmaxf(s.h, k.fr_vs);
-    float u = (wet ? s.hu : 0.0f) / safe;
-    float v = (wet ? s.hv : 0.0f) / safe;
+    float ys = shared_rcp(safe);
+    float u = quot(wet ? s.hu : 0.0f, safe, ys);
+    float v = quot(wet ? s.hv : 0.0f, safe, ys);
     float sp2 = u * u + v * v;
     bool moving = wet && (sp2 > 0.0f);
-    float speed = moving ? sqrtf(fmaxf(sp2, k.fr_e2)) : 0.0f;
+    float speed = moving ? root(fmaxf(sp2, k.fr_e2)) : 0.0f;
     float zz = fmaxf(z0, k.fr_e);
-    float ratio = fmaxf(s.h, k.fr_e) / zz;
-    float shallow = 1.0f / fmaxf(0.46f * ratio, k.fr_e);
+    float ratio = quot(fmaxf(s.h, k.fr_e), zz, shared_rcp(zz));
+    float shallow = recip(fmaxf(0.46f * ratio, k.fr_e));
     float rc = fmaxf(ratio, k.fr_e);
-    float lt = 2.5f * (((float)log((double)rc) - 1.0f) + (1.0f / rc) * 1.359f);
-    float deep = 1.0f / fmaxf(lt * lt, k.fr_e);
+    float lt = 2.5f * (((float)log((double)rc) - 1.0f) + recip(rc) * 1.359f);
+    float deep = recip(fmaxf(lt * lt, k.fr_e));
     float cf = ratio < 2.71828182845904523536f ? shallow : deep;
     return apply_friction_factor(s, cf, dt, k, speed, safe, wet);
 }

@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <stdlib.h>
+#include <string.h>
 
 #include "swe_common.cuh"
 
@@ -46,6 +48,8 @@ struct StepArgs {
     float* tend;   // stage 1: k1 output; stage 2: k1 input
     float* U_out;  // stage 2 output
     uint32_t* red;
+    const swe_clock* clk;  // device clock of forward(), or null for a plain step
+    float* hmax;           // running max depth [B,ny,nx], or null
     float max_dt, cval;
     int B, bedB, nB, levelB, ny, nx;
     int rain_mode, rain_batch, infil_mode, infil_batch;
@@ -166,11 +170,27 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
     const int b = blockIdx.z;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
 
+    if (a.clk != nullptr && !a.clk->active) {
+        // A step after the end of the call: the state is carried over unchanged.
+        if (STAGE == 2) {
+            const int j = j0 + tid / TX, i = i0 + tid % TX;
+            if (j < a.ny && i < a.nx) {
+                const size_t plane = (size_t)a.ny * a.nx;
+                const size_t o = at3(b, 0, j, i, a.ny, a.nx);
+                a.U_out[o] = a.U[o];
+                a.U_out[o + plane] = a.U[o + plane];
+                a.U_out[o + 2 * plane] = a.U[o + 2 * plane];
+            }
+        }
+        return;
+    }
+
     float dt = 0.0f, hdt = 0.0f;
     if (STAGE == 2) {
         // solver.py:620-626; torch.minimum propagates a NaN stable dt.
         const float st = stable_dt(u2f(a.red[0]), u2f(a.red[1]), kc);
-        dt = st != st ? st : fminf(st, a.max_dt);
+        const float max_dt = a.clk != nullptr ? a.clk->max_dt : a.max_dt;
+        dt = st != st ? st : fminf(st, max_dt);
         hdt = 0.5f * dt;
         if (tid == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
             uint32_t st_bits = 0;
@@ -282,6 +302,217 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
         a.U_out[o] = upd.h;
         a.U_out[o + plane] = upd.hu;
         a.U_out[o + 2 * plane] = upd.hv;
+        if (a.hmax != nullptr) {  // torch.maximum(hmax, U[:, 0]), NaN-propagating
+            float& m = a.hmax[at1(b, j, i, a.ny, a.nx)];
+            m = (upd.h > m || upd.h != upd.h) ? upd.h : m;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row-sweep form of the two stages.
+//
+// Each warp owns a strip of 32 columns -- 28 output columns plus the 2-cell
+// halo either side -- and SW_ROWS output rows, and sweeps down the strip one
+// row at a time.  The y-direction stencil lives in a rolling window of
+// registers (primitives of three rows, the previous y-face side and flux);
+// x-direction neighbours are exchanged with warp shuffles.  Per output cell
+// the warp computes one primitive, one x-side, one y-side, one x-face and
+// one y-face (plus 4/28 of a column and 4/SW_ROWS of a row of halo), with no
+// shared memory and no block barrier.
+constexpr int SW_OUT = 28;    // output columns per warp
+constexpr int SW_ROWS = 64;   // output rows per warp
+constexpr int SW_WARPS = 4;   // warps per block (side by side in x)
+
+// Cell (j, i) of the padded state for the sweep, ghost rules as region_cell;
+// also returns the raw U of an interior cell (for stage 2's corrector).
+template <int STAGE>
+__device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int i, float hdt,
+                                           State& s, float& z, State& uraw) {
+    const int ny = a.ny, nx = a.nx;
+    const bool jin = (unsigned)j < (unsigned)ny, iin = (unsigned)i < (unsigned)nx;
+    int js = min(max(j, 0), ny - 1), is = min(max(i, 0), nx - 1);
+    const bool xarm = jin && !iin && i >= -2 && i < nx + 2;
+    const bool yarm = iin && !jin && j >= -2 && j < ny + 2;
+    int code = -1, side = 0;
+    if (xarm || yarm) {
+        side = xarm ? (i < 0 ? 0 : 1) : (j < 0 ? 2 : 3);
+        code = a.bc[side];
+        if (code == SWE_BC_PERIODIC) {  // boundary.py:247-257, :301-302
+            if (xarm) is = i < 0 ? nx + i : i - nx;
+            else js = j < 0 ? ny + j : j - ny;
+        }
+    }
+    const size_t plane = (size_t)ny * nx;
+    const size_t o = at3(b, 0, js, is, ny, nx);
+    uraw = State{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
+    if (STAGE == 1) {
+        s = uraw;
+    } else {  // predictor clean(U, U + dt/2 k1), solver.py:639
+        const State c{uraw.h + hdt * a.tend[o], uraw.hu + hdt * a.tend[o + plane],
+                      uraw.hv + hdt * a.tend[o + 2 * plane]};
+        s = clean_and_limit(uraw, c, a.kc, a.positivity != 0);
+    }
+    z = bed_at(a, b, js, is);
+    if (code < 0 || code == SWE_BC_TRANSMISSIVE || code == SWE_BC_PERIODIC) return;
+    const float lev = a.level[a.levelB == 1 ? 0 : b];
+    if (code == SWE_BC_CONSTANT) {  // boundary.py:304-305
+        s = State{a.cval, a.cval, a.cval};
+    } else if (code == SWE_BC_WATER_LEVEL) {  // boundary.py:279-282, :307-310
+        s.h = fmaxf(lev - z, 0.0f);
+    } else if (code == SWE_BC_WALL) {  // boundary.py:312-316: flip of the first/last two lines
+        const int jm = xarm ? j : (j < 0 ? -1 - j : 2 * ny - 1 - j);
+        const int im = xarm ? (i < 0 ? -1 - i : 2 * nx - 1 - i) : i;
+        float mirror;
+        if (jm == js && im == is) {
+            mirror = xarm ? s.hu : s.hv;
+        } else {
+            State m = interior_state<STAGE>(a, b, jm, im, hdt);
+            mirror = xarm ? m.hu : m.hv;
+        }
+        if (xarm) s.hu = -mirror;
+        else s.hv = -mirror;
+    } else if (code == SWE_BC_ABSORBING) {  // boundary.py:318-328
+        const float hr = fmaxf(lev - z, 0.0f);
+        const float hg = s.h;
+        const float hc = hr > a.kc.absorb_lim ? hr : hg;
+        const float c = sqrtf(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
+        const float val = ((side == 0 || side == 2) ? -c : c) * (hg - hr);
+        if (xarm) s.hu = val;
+        else s.hv = val;
+    }
+}
+
+__device__ __forceinline__ float shfl_up1(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float shfl_dn1(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+template <int STAGE>
+__global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) {
+    const SweConsts& kc = a.kc;
+    const int lane = threadIdx.x & 31;
+    const int strip = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
+    const int i0 = strip * SW_OUT;
+    const int j0 = blockIdx.y * SW_ROWS;
+    const int b = blockIdx.z;
+    if (i0 >= a.nx) return;  // whole warp
+    const int c = i0 - 2 + lane;  // this lane's column
+    const bool out_lane = lane >= 2 && lane < 2 + SW_OUT && c < a.nx;
+    const int jend = min(j0 + SW_ROWS, a.ny);  // one past the last output row
+    const size_t plane = (size_t)a.ny * a.nx;
+
+    if (a.clk != nullptr && !a.clk->active) {
+        if (STAGE == 2 && out_lane)
+            for (int j = j0; j < jend; ++j) {
+                const size_t o = at3(b, 0, j, c, a.ny, a.nx);
+                a.U_out[o] = a.U[o];
+                a.U_out[o + plane] = a.U[o + plane];
+                a.U_out[o + 2 * plane] = a.U[o + 2 * plane];
+            }
+        return;
+    }
+
+    float dt = 0.0f, hdt = 0.0f;
+    if (STAGE == 2) {
+        const float st = stable_dt(u2f(a.red[0]), u2f(a.red[1]), kc);
+        const float max_dt = a.clk != nullptr ? a.clk->max_dt : a.max_dt;
+        dt = st != st ? st : fminf(st, max_dt);
+        hdt = 0.5f * dt;
+        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+            uint32_t st_bits = 0;
+            if (!isfinite(dt)) st_bits |= SWE_S_NONFINITE_DT;
+            else if (!(dt > 0.0f)) st_bits |= SWE_S_NONPOSITIVE_DT;
+            if (st_bits) atomicOr(&a.red[2], st_bits);
+            a.red[3] = f2u(dt);
+        }
+    }
+
+    const bool wsr = a.wsr != 0;
+    Prim pm2{}, pm1{}, p0{};      // primitives of rows k-2, k-1, k
+    State um2{}, um1{}, u0{};     // raw U of those rows (stage 2)
+    Side sy_prev_p{};              // "p" side of row k-2 in y
+    float fy_m = 0.0f, fy_nR = 0.0f, fy_t = 0.0f;  // face above row k-2
+    uint32_t axb = 0u, ayb = 0u;
+    bool bad = false;
+    for (int k = j0 - 2, it = 0; k < jend + 2; ++k, ++it) {
+        State s, ur;
+        float z;
+        sweep_cell<STAGE>(a, b, k, c, hdt, s, z, ur);
+        if (STAGE == 1 && (unsigned)k < (unsigned)a.ny && (unsigned)c < (unsigned)a.nx)
+            bad |= !(isfinite(s.h) && isfinite(s.hu) && isfinite(s.hv));
+        pm2 = pm1;
+        pm1 = p0;
+        p0 = make_prim(s.h, s.hu, s.hv, z, kc);
+        if (STAGE == 2) {
+            um2 = um1;
+            um1 = u0;
+            u0 = ur;
+        }
+        if (it < 2) continue;
+        // y-sides of row k-1 (reconstruction.py:26-96 along y)
+        const Sides sy = make_sides(pm2, pm1, p0, kc, wsr);
+        if (it >= 3) {
+            // y-face between rows k-2 and k-1
+            const FaceFlux fy = face_flux(sy_prev_p, pm2.h, pm2.z, sy.m, pm1.h, pm1.z, true, kc);
+            if (STAGE == 1 && out_lane && k - 1 >= 0 && k - 1 <= a.ny) ayb = max(ayb, fy.speed_bits);
+            if (it >= 4) {
+                // Output row o = k-2: its primitives are pm2.  x-sides need the
+                // neighbours' primitives, x-faces the right neighbour's side.
+                const int o = k - 2;
+                const Prim xl{shfl_up1(pm2.h), shfl_up1(pm2.u), shfl_up1(pm2.v), shfl_up1(pm2.eta),
+                              shfl_up1(pm2.z)};
+                const Prim xr{shfl_dn1(pm2.h), shfl_dn1(pm2.u), shfl_dn1(pm2.v), shfl_dn1(pm2.eta),
+                              shfl_dn1(pm2.z)};
+                const Sides sx = make_sides(xl, pm2, xr, kc, wsr);
+                const Side rm{shfl_dn1(sx.m.hlin), shfl_dn1(sx.m.eta), shfl_dn1(sx.m.bed),
+                              shfl_dn1(sx.m.u), shfl_dn1(sx.m.v)};
+                const FaceFlux fx = face_flux(sx.p, pm2.h, pm2.z, rm, xr.h, xr.z, false, kc);
+                if (STAGE == 1 && lane >= 1 && lane < 2 + SW_OUT && c >= -1 && c < a.nx)
+                    axb = max(axb, fx.speed_bits);
+                const FaceFlux fxl{shfl_up1(fx.fmass), 0.0f, shfl_up1(fx.fnorm_R), shfl_up1(fx.ftan), 0u};
+                const FaceFlux fyt{fy_m, 0.0f, fy_nR, fy_t, 0u};
+                if (out_lane) {
+                    const float rain = forcing(a.rain, a.rain_mode, a.rain_batch, b, o, c, a.ny, a.nx);
+                    const float loss =
+                        fmaxf(forcing(a.infil, a.infil_mode, a.infil_batch, b, o, c, a.ny, a.nx), 0.0f);
+                    const Rhs r = cell_rhs(fxl, fx, fyt, fy, kc, rain, loss);
+                    const size_t oo = at3(b, 0, o, c, a.ny, a.nx);
+                    if (STAGE == 1) {
+                        a.tend[oo] = r.r0;
+                        a.tend[oo + plane] = r.r1;
+                        a.tend[oo + 2 * plane] = r.r2;
+                    } else {
+                        const State u = um2;
+                        const State cand{u.h + dt * r.r0, u.hu + dt * r.r1, u.hv + dt * r.r2};
+                        State upd = clean_and_limit(u, cand, kc, a.positivity != 0);
+                        if (a.friction) {
+                            const float nv = a.n[at1(a.nB == 1 ? 0 : b, o, c, a.ny, a.nx)];
+                            upd = a.friction_model == 0 ? manning(upd, nv, dt, kc)
+                                                        : roughness_friction(upd, nv, dt, kc);
+                        }
+                        a.U_out[oo] = upd.h;
+                        a.U_out[oo + plane] = upd.hu;
+                        a.U_out[oo + 2 * plane] = upd.hv;
+                        if (a.hmax != nullptr) {
+                            float& m = a.hmax[at1(b, o, c, a.ny, a.nx)];
+                            m = (upd.h > m || upd.h != upd.h) ? upd.h : m;
+                        }
+                    }
+                }
+            }
+            fy_m = fy.fmass;
+            fy_nR = fy.fnorm_R;
+            fy_t = fy.ftan;
+        }
+        sy_prev_p = sy.p;
+    }
+    if (STAGE == 1) {
+        axb = warp_max_u32(axb);
+        ayb = warp_max_u32(ayb);
+        if (lane == 0) {
+            if (axb) atomicMax(&a.red[0], axb);
+            if (ayb) atomicMax(&a.red[1], ayb);
+        }
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&a.red[2], SWE_S_NONFINITE_STATE);
     }
 }
 
@@ -293,6 +524,7 @@ bool fill_common(StepArgs& a, const float* U, const float* bed, int B, int bedB,
     if (levelB != 1 && levelB != B) return false;
     if ((long long)ny * nx * 3 * B >= (1ll << 40)) return false;
     if ((ny + TY - 1) / TY > 65535 || B > 65535) return false;
+    if ((long long)((nx + SW_OUT - 1) / SW_OUT + SW_WARPS - 1) / SW_WARPS > 2147483647LL) return false;
     a.U = U;
     a.bed = bed;
     a.level = level;
@@ -324,6 +556,21 @@ bool valid_forcing(const float* f, int mode, int fb, int B) {
 
 dim3 grid_of(const StepArgs& a) { return dim3((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, a.B); }
 
+dim3 sweep_grid_of(const StepArgs& a) {
+    const int strips = (a.nx + SW_OUT - 1) / SW_OUT;
+    return dim3((strips + SW_WARPS - 1) / SW_WARPS, (a.ny + SW_ROWS - 1) / SW_ROWS, a.B);
+}
+
+// Kernel form of the two stages: the shared-memory tile form (default) or
+// the row sweep (SWE_STEP_KERNEL=sweep), read once per process.
+bool use_tiled_kernels() {
+    static const bool tiled = [] {
+        const char* v = getenv("SWE_STEP_KERNEL");
+        return !(v != nullptr && strcmp(v, "sweep") == 0);
+    }();
+    return tiled;
+}
+
 }  // namespace
 }  // namespace swe
 
@@ -352,12 +599,13 @@ extern "C" int swe_spatial_operator_f32(const float* U, const float* bed, int B,
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
-extern "C" int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB,
-                                  const float* n, int nB, int B, int ny, int nx,
-                                  const swe_params* p, const float* level, int levelB,
-                                  float max_dt, const float* infil, int infil_mode,
-                                  int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
-                                  void* stream) {
+namespace swe {
+namespace {
+
+int launch_step(int stage, const float* U, const float* bed, int bedB, const float* n, int nB, int B,
+                int ny, int nx, const swe_params* p, const float* level, int levelB, float max_dt,
+                const swe_clock* clk, const float* infil, int infil_mode, int infil_batch,
+                float* scratch_k, uint32_t* red, float* U_out, float* hmax, void* stream) {
     StepArgs a{};
     if (stage != 1 && stage != 2 && stage != 3) return SWE_EARG;
     if (!fill_common(a, U, bed, B, bedB, ny, nx, p, level, levelB)) return SWE_EARG;
@@ -374,14 +622,47 @@ extern "C" int swe_step_stage_f32(int stage, const float* U, const float* bed, i
     a.U_out = U_out;
     a.red = red;
     a.max_dt = max_dt;
+    a.clk = clk;
+    a.hmax = hmax;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 g = grid_of(a);
+    const bool tiled = use_tiled_kernels();
+    const dim3 g = tiled ? grid_of(a) : sweep_grid_of(a);
     if (stage & 1) {
-        if (cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
-        stage_kernel<1><<<g, NT, 0, s>>>(a);
+        // A clocked step's reduction words are cleared by swe_clock_f32.
+        if (!clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
+            return SWE_ECUDA;
+        if (tiled) stage_kernel<1><<<g, NT, 0, s>>>(a);
+        else sweep_kernel<1><<<g, SW_WARPS * 32, 0, s>>>(a);
     }
-    if (stage & 2) stage_kernel<2><<<g, NT, 0, s>>>(a);
+    if (stage & 2) {
+        if (tiled) stage_kernel<2><<<g, NT, 0, s>>>(a);
+        else sweep_kernel<2><<<g, SW_WARPS * 32, 0, s>>>(a);
+    }
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+}  // namespace
+}  // namespace swe
+
+extern "C" int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB,
+                                  const float* n, int nB, int B, int ny, int nx,
+                                  const swe_params* p, const float* level, int levelB,
+                                  float max_dt, const float* infil, int infil_mode,
+                                  int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                                  void* stream) {
+    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt, nullptr,
+                       infil, infil_mode, infil_batch, scratch_k, red, U_out, nullptr, stream);
+}
+
+extern "C" int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB,
+                                    const float* n, int nB, int B, int ny, int nx,
+                                    const swe_params* p, const float* level, int levelB,
+                                    const swe_clock* clock, const float* infil, int infil_mode,
+                                    int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                                    float* hmax, void* stream) {
+    if (!clock) return SWE_EARG;
+    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, 0.0f, clock, infil,
+                       infil_mode, infil_batch, scratch_k, red, U_out, hmax, stream);
 }
 
 extern "C" int swe_step_f32(const float* U, const float* bed, int bedB, const float* n, int nB,

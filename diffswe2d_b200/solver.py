@@ -324,6 +324,9 @@ class SWE2D(nn.Module):
             raise ValueError(f"t_end duration cannot be negative: {duration}.")
         if duration == 0.0:
             return U0, U0[:, 0].clone()
+        if self._device_loop_ok(U0, callback, boundary_level, max_dt_cap):
+            return self._forward_device(U0, duration, absolute_start, int(max_steps), infiltration,
+                                        boundary_level, max_dt_cap)
         U, hmax, elapsed = U0, U0[:, 0].clone(), 0.0
         tolerance = max(1e-12, 1e-12 * abs(duration))
         for iteration in range(max_steps):
@@ -347,6 +350,123 @@ class SWE2D(nn.Module):
                 callback(iteration, absolute_start + elapsed, U)
         raise RuntimeError(f"max_steps={max_steps} reached after {elapsed:.8f} s; "
                            f"requested duration={duration:.8f} s.")
+
+    # ------------------------------------------------ device-driven forward
+    #: steps per CUDA-graph replay of the device-driven loop (even: the state
+    #: ping-pongs between two buffers and ends each chunk in the first)
+    steps_per_chunk = 32
+
+    def _device_loop_ok(self, U0, callback, boundary_level, max_dt_cap) -> bool:
+        """The device loop serves forward() calls that need no host work per
+        step: no callback, no autograd, and a positive max_dt cap if any."""
+        if callback is not None or not U0.is_cuda or U0.dtype != torch.float32:
+            return False
+        if torch.is_grad_enabled() and (U0.requires_grad or (
+                torch.is_tensor(boundary_level) and boundary_level.requires_grad) or (
+                boundary_level is None and self.use_dynamic_bc and self.bc_wls.requires_grad)):
+            return False
+        if max_dt_cap is not None and not self._scalar_float(max_dt_cap, "max_dt_cap") > 0.0:
+            return False
+        return True
+
+    def _forward_device(self, U0, duration, absolute_start, max_steps, infiltration,
+                        boundary_level, max_dt_cap):
+        """forward() with the time loop on the device (src/solver.py:680-779).
+
+        Each chunk of ``steps_per_chunk`` steps is one CUDA-graph replay of
+        [stage 1, stage 2, clock] launches; the host reads the 72-byte clock
+        once per chunk.  Results are those of the host loop bit for bit.
+        """
+        self._check_state(U0)
+        U0 = nat.require_cuda_f32("U0", U0.detach())
+        dev = U0.device
+        B, _, ny, nx = U0.shape
+        bed, n = self._fields(U0)
+        series_t = series_w = None
+        nseries = 0
+        if boundary_level is not None:
+            lv, levelB = self._level_arg(self._prepare_boundary_level(boundary_level, U0), B)
+        elif self.use_dynamic_bc:
+            series_t = self.bc_times.detach().to(dtype=torch.float32, device=dev).contiguous()
+            series_w = self.bc_wls.detach().to(dtype=torch.float32, device=dev).contiguous()
+            nseries = series_t.numel()
+            lv, levelB = torch.zeros(1, dtype=torch.float32, device=dev), 1
+        else:
+            lv, levelB = self._level_arg(self._prepare_boundary_level(self.cfg.constant_level, U0), B)
+        infil, imode, iB = self._forcing_arg(infiltration, U0[:, 0:1])
+        bufs = [U0.clone(), torch.empty_like(U0)]
+        scratch = torch.empty_like(U0)
+        red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+        hmax = U0[:, 0].clone()
+        cap = self._scalar_float(max_dt_cap, "max_dt_cap") if max_dt_cap is not None else 0.0
+        clock_host = nat.SweClock(duration, absolute_start, max(1e-12, 1e-12 * abs(duration)),
+                                  cap, 0.0, max_steps, 0, 0, 0, 0, 0.0, 0.0, 0.0)
+        clock = torch.frombuffer(bytearray(bytes(clock_host)), dtype=torch.uint8).to(dev)
+        names = list(self.gauge_indices) if self.track_gauges else []
+        chunk = self.steps_per_chunk
+        cells = gbuf = None
+        if names:
+            idx = [self.gauge_indices[name] for name in names]
+            for iy, ix in idx:
+                if not (0 <= iy < ny and 0 <= ix < nx):
+                    raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
+            cells = torch.tensor(idx, dtype=torch.int32, device=dev).reshape(-1).contiguous()
+            gbuf = torch.zeros((chunk, 2 + len(names)), dtype=torch.float64, device=dev)
+        lib, p = nat.lib(), self._params()
+
+        def clock_tick(state):
+            rc = lib.swe_clock_f32(nat.ptr(clock), nat.ptr(red), nat.ptr(series_t), nat.ptr(series_w),
+                                   nseries, nat.ptr(lv), nat.ptr(state), ny, nx, nat.ptr(cells),
+                                   len(names), nat.ptr(gbuf), chunk if names else 0,
+                                   nat.stream_handle(dev))
+            nat.check(rc, "forward clock")
+
+        def one_step(src, dst):
+            rc = lib.swe_step_clocked_f32(3, nat.ptr(src), nat.ptr(bed), bed.shape[0], nat.ptr(n),
+                                          n.shape[0], B, ny, nx, p, nat.ptr(lv), levelB,
+                                          nat.ptr(clock), nat.ptr(infil), imode, iB,
+                                          nat.ptr(scratch), nat.ptr(red), nat.ptr(dst),
+                                          nat.ptr(hmax), nat.stream_handle(dev))
+            nat.check(rc, "forward step")
+            clock_tick(dst)
+
+        clock_tick(bufs[0])  # sets up the first step
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for s in range(chunk):
+                one_step(bufs[s % 2], bufs[1 - s % 2])
+        bed_at = None
+        if names:
+            bed0 = self.bed.detach()[0, 0]
+            bed_at = {name: float(bed0[iy, ix]) for name, (iy, ix) in zip(names, idx)}
+        steps_seen = 0
+        try:
+            while True:
+                graph.replay()
+                raw = clock.cpu().numpy().tobytes()
+                c = nat.SweClock.from_buffer_copy(raw)
+                if names and c.steps > steps_seen:
+                    rows = gbuf.cpu().numpy()
+                    for s in range(steps_seen, c.steps):
+                        r = rows[s % chunk]
+                        self.ts_time.append(float(r[0]))
+                        self.ts_dt.append(float(r[1]))
+                        for g, name in enumerate(names):
+                            depth = float(r[2 + g])
+                            self.ts_h.setdefault(name, []).append(depth)
+                            self.ts_z.setdefault(name, []).append(depth + bed_at[name])
+                steps_seen = c.steps
+                if c.state == nat.CLOCK_FAILED:
+                    self._raise_on_status(c.dt_status, float(c.last_dt))
+                if c.state == nat.CLOCK_DONE:
+                    break
+                if c.state == nat.CLOCK_MAXSTEPS:
+                    raise RuntimeError(f"max_steps={max_steps} reached after {c.elapsed:.8f} s; "
+                                       f"requested duration={duration:.8f} s.")
+        finally:
+            del graph
+        self.last_forward_steps = steps_seen
+        return bufs[0], hmax
 
     def _record_gauges(self, U: torch.Tensor, absolute_time: float, dt_value: float) -> None:
         """Micro-step gauge records (src/solver.py:781-801)."""

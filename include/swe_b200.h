@@ -107,6 +107,67 @@ int swe_step_stage_f32(int stage, const float* U, const float* bed, int bedB, co
                        int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                        void* stream);
 
+/* ---------------------------------------------------------------------
+ * Device-driven time loop (SWE2D.forward, src/solver.py:680-779).
+ * --------------------------------------------------------------------- */
+
+/* Clock of one forward() call, kept in device memory.  The host fills the
+ * first six fields (and zeroes the rest) before the first swe_clock_f32;
+ * the device advances it one step at a time, in double precision, exactly
+ * as the reference's Python loop does. */
+typedef struct swe_clock {
+    double duration;   /* t_end of the call (a duration)                      */
+    double start;      /* absolute start time                                 */
+    double tolerance;  /* max(1e-12, 1e-12 |duration|), solver.py:739          */
+    double max_dt_cap; /* > 0: cap on each step's max_dt (solver.py:748-749)   */
+    double elapsed;    /* time advanced so far                                 */
+    int32_t max_steps; /* RuntimeError bound, solver.py:741, :776-779          */
+    int32_t steps;     /* steps taken                                          */
+    int32_t active;    /* the next step runs                                   */
+    int32_t state;     /* SWE_CLOCK_* below                                    */
+    uint32_t dt_status;/* status bits of the failed step (SWE_S_*)             */
+    float max_dt;      /* float32 max_dt of the next step                      */
+    float level;       /* interpolated boundary level of the next step         */
+    float last_dt;     /* dt of the last step taken                            */
+} swe_clock;
+
+#define SWE_CLOCK_RUNNING 0
+#define SWE_CLOCK_DONE 1      /* remaining time <= tolerance                   */
+#define SWE_CLOCK_MAXSTEPS 2  /* max_steps taken before the duration elapsed    */
+#define SWE_CLOCK_FAILED 3    /* a step raised (dt_status holds SWE_S_* bits)   */
+
+/*
+ * swe_clock_f32: the bookkeeping between two steps of forward().  If the
+ * previous step ran: read its dt and status from red, elapsed += dt with
+ * the end-of-call clamp (solver.py:766-768), steps += 1, and record the
+ * depth of batch 0 at the ngauge cells gauge_cells[2*g], gauge_cells[2*g+1]
+ * (row, column) of U into the ring gauges[row*(2+ngauge)+...] as (absolute
+ * time, dt, depths...) with row = (steps - 1) % gauge_rows
+ * (SWE2D._record_gauges, solver.py:781-801).  Then set up the next step:
+ * stop when max_steps steps are taken or the remaining time is within
+ * tolerance (solver.py:741-744), else max_dt = remaining (capped), and when nseries
+ * > 0 the boundary level at the current time interpolated from the series
+ * (SWE2D._interpolate_dynamic_boundary, solver.py:391-415) into *level_out;
+ * clear the reduction words of red.  One block; no host synchronisation.
+ */
+int swe_clock_f32(swe_clock* clock, uint32_t* red, const float* series_t, const float* series_w,
+                  int nseries, float* level_out, const float* U, int ny, int nx,
+                  const int32_t* gauge_cells, int ngauge, double* gauges, int gauge_rows,
+                  void* stream);
+
+/*
+ * One stage (1, 2 or 3 = both) of a step driven by a device clock: like
+ * swe_step_stage_f32 but max_dt comes from clock->max_dt and a step whose
+ * clock is not active does nothing except copy U to U_out in stage 2.  The
+ * reduction words are cleared by swe_clock_f32, not here.  hmax (optional,
+ * [B,ny,nx]) receives max(hmax, h_new) (solver.py:765).
+ */
+int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB, const float* n,
+                         int nB, int B, int ny, int nx, const swe_params* p, const float* level,
+                         int levelB, const swe_clock* clock, const float* infil, int infil_mode,
+                         int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                         float* hmax, void* stream);
+
 /*
  * swe_step_noalloc_f32 -- one step like swe_step_f32, for callers that must
  * not allocate device memory.  No counterpart in the reference: it exists
@@ -199,6 +260,20 @@ int swe_clean_and_limit_f32(const float* old, const float* cand, int B, int ny, 
  */
 int swe_friction_f32(const float* U, const float* n, int nB, int B, int ny, int nx, float dt,
                      int model, const swe_params* p, float* out, void* stream);
+
+/*
+ * Device self-test of the step's division and square root (no counterpart
+ * in the reference; it checks that the step's arithmetic is the IEEE
+ * correctly-rounded arithmetic of the reference's float32 tensors).
+ * which = 0: reciprocal, exhaustive over |b| in [2^-100, 2^100);
+ * which = 1: division on n random operand pairs (seed);
+ * which = 2: division on n operand pairs built next to rounding midpoints;
+ * which = 3: square root, exhaustive over [2^-100, 2^100).
+ * count (device, 1 x u64) receives the number of mismatches against CUDA's
+ * rcp.rn / div.rn / sqrt.rn, first (device, 2 x u32) the first bad input.
+ */
+int swe_selftest_arith_f32(int which, long long n, unsigned long long seed,
+                           unsigned long long* count, uint32_t* first, void* stream);
 
 #ifdef __cplusplus
 }

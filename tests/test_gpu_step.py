@@ -169,6 +169,61 @@ def test_forward_chunk(golden):
     assert np.array_equal(_np(hmax), d["fwcr_hmax"])
 
 
+def _runup_model(golden):
+    d = golden("c2_runup")
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall")
+    m = _model(d["bed"], d["n"], float(d["dx"]), float(d["dx"]), cfg)
+    m.set_dynamic_boundary(_t(d["bc_times"]), _t(d["bc_levels"]))
+    return d, m
+
+
+def test_forward_device_loop_bitwise(golden):
+    """forward() without a callback runs the time loop on the device (CUDA
+    graph chunks); same state, hmax and step count as the reference's loop."""
+    d, m = _runup_model(golden)
+    with torch.no_grad():
+        U, hmax = m(_t(d["f32cr_200"]), t_end=0.2, start_time=1.0)
+    assert m.last_forward_steps == len(d["fwcr_times"])
+    assert np.array_equal(_np(U), d["fwcr_U"])
+    assert np.array_equal(_np(hmax), d["fwcr_hmax"])
+
+
+def test_forward_device_loop_gauges_match_host_loop(golden):
+    d, m = _runup_model(golden)
+    gauges = {"g0": (30, 40), "g1": (122, 3), "g2": (200, 380)}
+    records = []
+    for use_callback in (True, False):
+        m.track_gauges = True
+        m.gauge_indices = dict(gauges)
+        m.reset_gauge_tracking()
+        cb = (lambda it, t, U: None) if use_callback else None
+        with torch.no_grad():
+            U, hmax = m(_t(d["U0"]), t_end=0.25, start_time=0.0, callback=cb)
+        records.append((list(m.ts_time), list(m.ts_dt), dict(m.ts_h), dict(m.ts_z), _np(U)))
+    host, dev = records
+    assert host[0] == dev[0] and host[1] == dev[1]
+    assert host[2] == dev[2] and host[3] == dev[3]
+    assert np.array_equal(host[4], dev[4])
+    assert len(dev[0]) > 40  # more than one graph chunk
+
+
+def test_forward_device_loop_errors(golden):
+    d, m = _runup_model(golden)
+    with torch.no_grad():
+        with pytest.raises(RuntimeError, match="max_steps=5 reached"):
+            m(_t(d["U0"]), t_end=10.0, max_steps=5)
+        U = _t(d["U0"]).clone()
+        U[0, 0, 100, 100] = float("nan")
+        with pytest.raises(FloatingPointError, match="non-finite"):
+            m(U, t_end=0.1)
+        # a cap on max_dt (solver.py:748-749) and an explicit level
+        U1, _ = m(_t(d["U0"]), t_end=0.05, max_dt_cap=1e-3, boundary_level=0.004)
+        U2, _ = m(_t(d["U0"]), t_end=0.05, max_dt_cap=1e-3, boundary_level=0.004,
+                  callback=lambda it, t, U: None)
+        assert torch.equal(U1, U2)
+
+
 def test_step_raises_like_reference():
     bed = torch.full((8, 8), -1.0, device=DEV)
     m = SWE2D(bed, torch.full_like(bed, 0.02), 1.0, 1.0, config=SWEConfig(), train_dem=False)
