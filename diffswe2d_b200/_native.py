@@ -89,6 +89,10 @@ _SIGNATURES = {
     "swe_clock_f32": [_P, _P, _P, _P, _I, _P, _P, _I, _I, _P, _I, _P, _I, _P],
     "swe_step_clocked_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _P, _P, _I, _I, _P, _P, _P, _P, _P],
+    "swe_adj_spatial_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _P, _P,
+                            _P, _P, _I, _P],
+    "swe_adj_pointwise_f32": [_I, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _F, _P,
+                              _P, _P, _P, _P, _P],
     "swe_step_noalloc_f32": [_P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _F, _P, _I, _I, _P, _P, _P],
     "swe_ghost_cells_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _I,

@@ -57,6 +57,15 @@ struct SweConsts {
 // rcp.rn for every float in the range used and div_by against div.rn on
 // random and near-halfway operands.  Quotients outside [2^-100, 2^100]
 // (zero excepted) and non-finite operands take the IEEE division instead.
+#if defined(__CUDA_ARCH__)
+// IEEE fallbacks for operands outside the range the fast forms are checked
+// for.  Out of line: one copy shared by every call site keeps the kernels'
+// code small (the branch to them is almost never taken).
+__device__ __noinline__ float ieee_div_slow(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __noinline__ float ieee_rcp_slow(float b) { return __frcp_rn(b); }
+__device__ __noinline__ float ieee_sqrt_slow(float x) { return __fsqrt_rn(x); }
+#endif
+
 SWE_HD float rcp_cr(float b) {
 #if defined(__CUDA_ARCH__)
     float y0;
@@ -64,7 +73,7 @@ SWE_HD float rcp_cr(float b) {
     const float e = __fmaf_rn(-b, y0, 1.0f);
     const float y1 = __fmaf_rn(y0, e, y0);
     const float ab = fabsf(b);
-    return (ab >= 0x1p-100f && ab < 0x1p+100f) ? y1 : __frcp_rn(b);
+    return (ab >= 0x1p-100f && ab < 0x1p+100f) ? y1 : ieee_rcp_slow(b);
 #else
     return 1.0f / b;
 #endif
@@ -78,7 +87,7 @@ SWE_HD float div_by(float a, float b, float y) {
     const float q1 = __fmaf_rn(r, y, q);
     const float aq = fabsf(q);
     const bool safe = (aq >= 0x1p-100f && aq <= 0x1p+100f) || a == 0.0f;
-    return safe ? q1 : __fdiv_rn(a, b);
+    return safe ? q1 : ieee_div_slow(a, b);
 #else
     (void)y;
     return a / b;
@@ -100,7 +109,7 @@ SWE_HD float sqrt_cr(float x) {
     const float r = __fmaf_rn(-s, s, x);
     const float s1 = __fmaf_rn(r, h, s);
     const bool safe = x >= 0x1p-100f && x < 0x1p+100f;
-    return safe ? s1 : __fsqrt_rn(x);
+    return safe ? s1 : ieee_sqrt_slow(x);
 #else
     return sqrtf(x);
 #endif

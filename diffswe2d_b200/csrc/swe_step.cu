@@ -50,6 +50,7 @@ struct StepArgs {
     uint32_t* red;
     const swe_clock* clk;  // device clock of forward(), or null for a plain step
     float* hmax;           // running max depth [B,ny,nx], or null
+    int rows;              // output rows per sweep tile
     float max_dt, cval;
     int B, bedB, nB, levelB, ny, nx;
     int rain_mode, rain_batch, infil_mode, infil_batch;
@@ -326,7 +327,33 @@ constexpr int SW_WARPS = 4;   // warps per block (side by side in x)
 
 // Cell (j, i) of the padded state for the sweep, ghost rules as region_cell;
 // also returns the raw U of an interior cell (for stage 2's corrector).
-template <int STAGE>
+// Loads of the state and the tendency.  CG = true bypasses L1 (ld.global.cg):
+// needed when another block of the same launch wrote the data (the
+// persistent ensemble kernel), since L1 is not coherent across blocks.
+template <bool CG>
+__device__ __forceinline__ float ld_state(const float* p) {
+    return CG ? __ldcg(p) : *p;
+}
+
+// The second source cell of a wall ghost two cells out (rare: domain edge
+// only), kept out of line to keep the sweep kernels' code small.
+template <int STAGE, bool CG>
+__device__ __noinline__ State mirror_state(const float* __restrict__ U, const float* __restrict__ tend,
+                                           int ny, int nx, int b, int j, int i, float hdt, float eps,
+                                           float dry, int positivity) {
+    const size_t plane = (size_t)ny * nx;
+    const size_t o = at3(b, 0, j, i, ny, nx);
+    const State u{ld_state<CG>(U + o), ld_state<CG>(U + o + plane), ld_state<CG>(U + o + 2 * plane)};
+    if (STAGE == 1) return u;
+    const State c{u.h + hdt * ld_state<CG>(tend + o), u.hu + hdt * ld_state<CG>(tend + o + plane),
+                  u.hv + hdt * ld_state<CG>(tend + o + 2 * plane)};
+    SweConsts k{};
+    k.eps = eps;
+    k.dry = dry;
+    return clean_and_limit(u, c, k, positivity != 0);
+}
+
+template <int STAGE, bool CG>
 __device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int i, float hdt,
                                            State& s, float& z, State& uraw) {
     const int ny = a.ny, nx = a.nx;
@@ -345,17 +372,17 @@ __device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int 
     }
     const size_t plane = (size_t)ny * nx;
     const size_t o = at3(b, 0, js, is, ny, nx);
-    uraw = State{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
+    uraw = State{ld_state<CG>(a.U + o), ld_state<CG>(a.U + o + plane), ld_state<CG>(a.U + o + 2 * plane)};
     if (STAGE == 1) {
         s = uraw;
     } else {  // predictor clean(U, U + dt/2 k1), solver.py:639
-        const State c{uraw.h + hdt * a.tend[o], uraw.hu + hdt * a.tend[o + plane],
-                      uraw.hv + hdt * a.tend[o + 2 * plane]};
+        const State c{uraw.h + hdt * ld_state<CG>(a.tend + o), uraw.hu + hdt * ld_state<CG>(a.tend + o + plane),
+                      uraw.hv + hdt * ld_state<CG>(a.tend + o + 2 * plane)};
         s = clean_and_limit(uraw, c, a.kc, a.positivity != 0);
     }
     z = bed_at(a, b, js, is);
     if (code < 0 || code == SWE_BC_TRANSMISSIVE || code == SWE_BC_PERIODIC) return;
-    const float lev = a.level[a.levelB == 1 ? 0 : b];
+    const float lev = ld_state<CG>(a.level + (a.levelB == 1 ? 0 : b));
     if (code == SWE_BC_CONSTANT) {  // boundary.py:304-305
         s = State{a.cval, a.cval, a.cval};
     } else if (code == SWE_BC_WATER_LEVEL) {  // boundary.py:279-282, :307-310
@@ -367,7 +394,8 @@ __device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int 
         if (jm == js && im == is) {
             mirror = xarm ? s.hu : s.hv;
         } else {
-            State m = interior_state<STAGE>(a, b, jm, im, hdt);
+            const State m = mirror_state<STAGE, CG>(a.U, a.tend, ny, nx, b, jm, im, hdt, a.kc.eps,
+                                                    a.kc.dry, a.positivity);
             mirror = xarm ? m.hu : m.hv;
         }
         if (xarm) s.hu = -mirror;
@@ -386,18 +414,21 @@ __device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int 
 __device__ __forceinline__ float shfl_up1(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ float shfl_dn1(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-template <int STAGE>
-__global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) {
+// FRIC: 0 no friction, 1 Manning, 2 roughness length (stage 2 only).
+// One tile of the sweep: SW_WARPS strips side by side (tile column bx) times
+// `rows` output rows (tile row by) of batch member b.  The whole block calls
+// it; warps whose strip lies beyond the grid return at once.
+template <int STAGE, int FRIC, bool CG>
+__device__ __forceinline__ void sweep_tile(const StepArgs& a, int bx, int by, int b, int rows) {
     const SweConsts& kc = a.kc;
     const int lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
+    const int strip = bx * SW_WARPS + (threadIdx.x >> 5);
     const int i0 = strip * SW_OUT;
-    const int j0 = blockIdx.y * SW_ROWS;
-    const int b = blockIdx.z;
+    const int j0 = by * rows;
     if (i0 >= a.nx) return;  // whole warp
     const int c = i0 - 2 + lane;  // this lane's column
     const bool out_lane = lane >= 2 && lane < 2 + SW_OUT && c < a.nx;
-    const int jend = min(j0 + SW_ROWS, a.ny);  // one past the last output row
+    const int jend = min(j0 + rows, a.ny);  // one past the last output row
     const size_t plane = (size_t)a.ny * a.nx;
 
     if (a.clk != nullptr && !a.clk->active) {
@@ -413,11 +444,13 @@ __global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) 
 
     float dt = 0.0f, hdt = 0.0f;
     if (STAGE == 2) {
-        const float st = stable_dt(u2f(a.red[0]), u2f(a.red[1]), kc);
+        const uint32_t ax = CG ? __ldcg(a.red) : a.red[0];
+        const uint32_t ay = CG ? __ldcg(a.red + 1) : a.red[1];
+        const float st = stable_dt(u2f(ax), u2f(ay), kc);
         const float max_dt = a.clk != nullptr ? a.clk->max_dt : a.max_dt;
         dt = st != st ? st : fminf(st, max_dt);
         hdt = 0.5f * dt;
-        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+        if (threadIdx.x == 0 && bx == 0 && by == 0 && b == 0) {
             uint32_t st_bits = 0;
             if (!isfinite(dt)) st_bits |= SWE_S_NONFINITE_DT;
             else if (!(dt > 0.0f)) st_bits |= SWE_S_NONPOSITIVE_DT;
@@ -436,7 +469,7 @@ __global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) 
     for (int k = j0 - 2, it = 0; k < jend + 2; ++k, ++it) {
         State s, ur;
         float z;
-        sweep_cell<STAGE>(a, b, k, c, hdt, s, z, ur);
+        sweep_cell<STAGE, CG>(a, b, k, c, hdt, s, z, ur);
         if (STAGE == 1 && (unsigned)k < (unsigned)a.ny && (unsigned)c < (unsigned)a.nx)
             bad |= !(isfinite(s.h) && isfinite(s.hu) && isfinite(s.hv));
         pm2 = pm1;
@@ -484,17 +517,17 @@ __global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) 
                         const State u = um2;
                         const State cand{u.h + dt * r.r0, u.hu + dt * r.r1, u.hv + dt * r.r2};
                         State upd = clean_and_limit(u, cand, kc, a.positivity != 0);
-                        if (a.friction) {
+                        if (FRIC != 0) {
                             const float nv = a.n[at1(a.nB == 1 ? 0 : b, o, c, a.ny, a.nx)];
-                            upd = a.friction_model == 0 ? manning(upd, nv, dt, kc)
-                                                        : roughness_friction(upd, nv, dt, kc);
+                            upd = FRIC == 1 ? manning(upd, nv, dt, kc) : roughness_friction(upd, nv, dt, kc);
                         }
                         a.U_out[oo] = upd.h;
                         a.U_out[oo + plane] = upd.hu;
                         a.U_out[oo + 2 * plane] = upd.hv;
                         if (a.hmax != nullptr) {
-                            float& m = a.hmax[at1(b, o, c, a.ny, a.nx)];
-                            m = (upd.h > m || upd.h != upd.h) ? upd.h : m;
+                            float* mp = a.hmax + at1(b, o, c, a.ny, a.nx);
+                            const float m = ld_state<CG>(mp);
+                            *mp = (upd.h > m || upd.h != upd.h) ? upd.h : m;
                         }
                     }
                 }
@@ -515,6 +548,214 @@ __global__ void __launch_bounds__(SW_WARPS * 32) sweep_kernel(const StepArgs a) 
         if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&a.red[2], SWE_S_NONFINITE_STATE);
     }
 }
+
+template <int STAGE, int FRIC>
+__global__ void __launch_bounds__(SW_WARPS * 32, STAGE == 2 ? 6 : 8) sweep_kernel(const StepArgs a) {
+    sweep_tile<STAGE, FRIC, false>(a, blockIdx.x, blockIdx.y, blockIdx.z, a.rows);
+}
+
+
+// ---------------------------------------------------------------------------
+// Persistent ensemble kernel: many independent scenarios of different grid
+// sizes, each with its own time step, boundary series and step count, in
+// one launch.
+//
+// Work item = (scenario, phase, tile); phase 2n is stage 1 of step n, phase
+// 2n+1 its stage 2.  Each scenario keeps a 64-bit claim word (phase << 32 |
+// tiles claimed) and a done counter.  A block claims a tile with one
+// atomicAdd on the claim word; when the phase is fully claimed it tries the
+// next scenario.  The block that completes a phase's last tile advances the
+// scenario (time, step count, next boundary level, cleared reductions) and
+// publishes the next phase with atomicExch.  No block ever waits for a
+// particular item, so the kernel cannot deadlock; idle polling is bounded
+// (EnsIdleLimit polls with __nanosleep back-off) after which the kernel sets
+// an error bit and returns.  State written by other blocks is read through
+// L2 (ld.global.cg); writes are fenced before a phase is published.
+struct EnsCtl {
+    unsigned long long claim;  // phase << 32 | tiles claimed
+    unsigned int done;         // tiles finished in the current phase
+    unsigned int red[SWE_RED_WORDS];
+    float level;               // boundary level of the current step
+    int step;                  // steps completed
+    int finished;              // 0 running, 1 done, 2 failed
+    int tiles, nbx, rows, steps;
+    int nseries;
+    float dt_last;
+    unsigned int status;
+    double time;               // simulated time since the start
+    double start;
+    const float* series_t;
+    const float* series_w;
+    float* Ua;                 // state buffers: step n reads U[n & 1]
+    float* Ub;
+};
+
+struct EnsGlobal {
+    unsigned int finished;  // scenarios done or failed
+    unsigned int error;     // bit 1: idle limit reached
+    unsigned int pad[14];
+};
+
+constexpr unsigned int EnsIdleLimit = 1u << 22;
+
+__device__ float ens_level(const EnsCtl& c) {
+    if (c.nseries <= 0) return c.level;
+    const float t = (float)(c.start + c.time);
+    const float* times = c.series_t;
+    const float* levels = c.series_w;
+    const int n = c.nseries;
+    if (n == 1) return levels[0];
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (times[mid] < t) lo = mid + 1;
+        else hi = mid;
+    }
+    const int idx = min(max(lo, 1), n - 1);
+    const float t0 = times[idx - 1], t1 = times[idx];
+    const float weight = __fdiv_rn(t - t0, fmaxf(t1 - t0, 1.1920929e-07f));
+    return levels[idx - 1] + weight * (levels[idx] - levels[idx - 1]);
+}
+
+// Thread 0 of the block that finished the last tile of `phase`.
+__device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
+    __threadfence();
+    c->done = 0u;
+    const unsigned int st = __ldcg(&c->red[2]);
+    if ((phase & 1u) == 0u) {  // stage 1 done: stage 2 derives dt from red
+        if (st & SWE_S_NONFINITE_STATE) {
+            c->status = st;
+            c->finished = 2;
+            __threadfence();
+            atomicAdd(&g->finished, 1u);
+            return;
+        }
+    } else {  // stage 2 done: the step is complete
+        const float dt = __uint_as_float(__ldcg(&c->red[3]));
+        if (st & (SWE_S_NONFINITE_DT | SWE_S_NONPOSITIVE_DT)) {
+            c->status = st;
+            c->finished = 2;
+            __threadfence();
+            atomicAdd(&g->finished, 1u);
+            return;
+        }
+        c->time += (double)dt;
+        c->dt_last = dt;
+        c->step += 1;
+        if (c->step >= c->steps) {
+            c->finished = 1;
+            __threadfence();
+            atomicAdd(&g->finished, 1u);
+            return;
+        }
+        c->level = ens_level(*c);
+        for (int w = 0; w < SWE_RED_WORDS; ++w) c->red[w] = 0u;
+    }
+    __threadfence();
+    atomicExch(&c->claim, (unsigned long long)(phase + 1u) << 32);
+}
+
+template <int FRIC>
+__global__ void __launch_bounds__(SW_WARPS * 32, 6)
+ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGlobal* g) {
+    __shared__ StepArgs sa;
+    __shared__ int s_item[3];
+    int rr = (int)(blockIdx.x % (unsigned)count);
+    unsigned int idle = 0;
+    while (true) {
+        __syncthreads();  // everyone is done with the previous item's shared data
+        if (threadIdx.x == 0) {
+            int item = -2, phase = 0, tile = 0;
+            for (int k = 0; k < count && item == -2; ++k) {
+                const int sidx = (rr + k) % count;
+                EnsCtl* c = ctl + sidx;
+                if (*(volatile int*)&c->finished) continue;
+                const unsigned long long old = atomicAdd(&c->claim, 1ull);
+                const unsigned int ph = (unsigned int)(old >> 32), cl = (unsigned int)old;
+                if (cl < (unsigned int)c->tiles) {
+                    item = sidx;
+                    phase = (int)ph;
+                    tile = (int)cl;
+                    rr = sidx;
+                }
+            }
+            if (item == -2) {
+                if (*(volatile unsigned int*)&g->finished >= (unsigned int)count ||
+                    *(volatile unsigned int*)&g->error) {
+                    item = -1;
+                } else if (++idle > EnsIdleLimit) {
+                    atomicOr(&g->error, 1u);
+                    item = -1;
+                } else {
+                    __nanosleep(256);
+                }
+            } else {
+                idle = 0;
+                __threadfence();
+            }
+            s_item[0] = item;
+            s_item[1] = phase;
+            s_item[2] = tile;
+        }
+        __syncthreads();
+        const int sidx = s_item[0];
+        if (sidx == -1) return;
+        if (sidx == -2) continue;
+        const int phase = s_item[1], tile = s_item[2];
+        // this scenario's arguments, with the state buffers of this step
+        {
+            const int* src = reinterpret_cast<const int*>(args + sidx);
+            int* dst = reinterpret_cast<int*>(&sa);
+            for (int w = threadIdx.x; w < (int)(sizeof(StepArgs) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+        }
+        __syncthreads();
+        const EnsCtl* c = ctl + sidx;
+        const int step = phase >> 1;
+        if (threadIdx.x == 0) {
+            sa.U = (step & 1) ? c->Ub : c->Ua;
+            sa.U_out = (step & 1) ? c->Ua : c->Ub;
+        }
+        __syncthreads();
+        const int nbx = c->nbx, rows = c->rows;
+        const int bx = tile % nbx, by = tile / nbx;
+        if ((phase & 1) == 0) sweep_tile<1, 0, true>(sa, bx, by, 0, rows);
+        else sweep_tile<2, FRIC, true>(sa, bx, by, 0, rows);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            EnsCtl* cw = ctl + sidx;
+            const unsigned int d = atomicAdd(&cw->done, 1u);
+            if (d + 1u == (unsigned int)cw->tiles) ens_advance(cw, g, (unsigned int)phase);
+        }
+    }
+}
+
+// One block of >= count threads (count <= 1024).
+__global__ void ensemble_init_kernel(EnsCtl* ctl, int count, EnsGlobal* g) {
+    const int t = threadIdx.x;
+    if (t == 0) {
+        g->finished = 0u;
+        g->error = 0u;
+    }
+    __syncthreads();
+    if (t < count) {
+        EnsCtl* c = ctl + t;
+        c->claim = 0ull;
+        c->done = 0u;
+        for (int w = 0; w < SWE_RED_WORDS; ++w) c->red[w] = 0u;
+        c->step = 0;
+        c->finished = c->steps > 0 ? 0 : 1;
+        c->status = 0u;
+        c->time = 0.0;
+        c->dt_last = 0.0f;
+        c->level = ens_level(*c);
+        if (c->finished) atomicAdd(&g->finished, 1u);
+    }
+}
+
+// Output rows per sweep tile for the single-grid kernels (tuning knob set by
+// swe_tune_sweep_rows; the ensemble carries one value per scenario).
+int g_sweep_rows = SW_ROWS;
 
 bool fill_common(StepArgs& a, const float* U, const float* bed, int B, int bedB, int ny, int nx,
                  const swe_params* p, const float* level, int levelB) {
@@ -543,6 +784,7 @@ bool fill_common(StepArgs& a, const float* U, const float* bed, int B, int bedB,
     a.friction = p->apply_friction;
     a.friction_model = p->friction_model;
     a.kc = make_consts(*p);
+    a.rows = g_sweep_rows;
     return true;
 }
 
@@ -558,15 +800,15 @@ dim3 grid_of(const StepArgs& a) { return dim3((a.nx + TX - 1) / TX, (a.ny + TY -
 
 dim3 sweep_grid_of(const StepArgs& a) {
     const int strips = (a.nx + SW_OUT - 1) / SW_OUT;
-    return dim3((strips + SW_WARPS - 1) / SW_WARPS, (a.ny + SW_ROWS - 1) / SW_ROWS, a.B);
+    return dim3((strips + SW_WARPS - 1) / SW_WARPS, (a.ny + a.rows - 1) / a.rows, a.B);
 }
 
-// Kernel form of the two stages: the shared-memory tile form (default) or
-// the row sweep (SWE_STEP_KERNEL=sweep), read once per process.
+// Kernel form of the two stages: the row sweep (default) or the
+// shared-memory tile form (SWE_STEP_KERNEL=tiled), read once per process.
 bool use_tiled_kernels() {
     static const bool tiled = [] {
         const char* v = getenv("SWE_STEP_KERNEL");
-        return !(v != nullptr && strcmp(v, "sweep") == 0);
+        return v != nullptr && strcmp(v, "tiled") == 0;
     }();
     return tiled;
 }
@@ -632,11 +874,18 @@ int launch_step(int stage, const float* U, const float* bed, int bedB, const flo
         if (!clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
             return SWE_ECUDA;
         if (tiled) stage_kernel<1><<<g, NT, 0, s>>>(a);
-        else sweep_kernel<1><<<g, SW_WARPS * 32, 0, s>>>(a);
+        else sweep_kernel<1, 0><<<g, SW_WARPS * 32, 0, s>>>(a);
     }
     if (stage & 2) {
-        if (tiled) stage_kernel<2><<<g, NT, 0, s>>>(a);
-        else sweep_kernel<2><<<g, SW_WARPS * 32, 0, s>>>(a);
+        if (tiled) {
+            stage_kernel<2><<<g, NT, 0, s>>>(a);
+        } else if (!a.friction) {
+            sweep_kernel<2, 0><<<g, SW_WARPS * 32, 0, s>>>(a);
+        } else if (a.friction_model == 0) {
+            sweep_kernel<2, 1><<<g, SW_WARPS * 32, 0, s>>>(a);
+        } else {
+            sweep_kernel<2, 2><<<g, SW_WARPS * 32, 0, s>>>(a);
+        }
     }
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
@@ -731,5 +980,142 @@ extern "C" int swe_step_noalloc_f32(const float* U, const float* bed, int bedB, 
     if (cudaMemcpyAsync(status_dt, red + 2, 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                         (cudaStream_t)stream) != cudaSuccess)
         return SWE_ECUDA;
+    return SWE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble entry points.
+namespace swe {
+namespace {
+
+size_t ens_offset_ctl(int count) { return ((size_t)count * sizeof(StepArgs) + 255) / 256 * 256; }
+size_t ens_offset_global(int count) {
+    return ens_offset_ctl(count) + ((size_t)count * sizeof(EnsCtl) + 255) / 256 * 256;
+}
+
+}  // namespace
+}  // namespace swe
+
+extern "C" long long swe_ensemble_workspace_bytes(int count) {
+    if (count < 1 || count > 1024) return -1;
+    return (long long)(ens_offset_global(count) + sizeof(EnsGlobal));
+}
+
+extern "C" int swe_ensemble_prepare_f32(const swe_ensemble_member* members, int count,
+                                        void* workspace, void* stream) {
+    if (!members || !workspace || count < 1 || count > 1024) return SWE_EARG;
+    StepArgs* args = (StepArgs*)malloc(sizeof(StepArgs) * count);
+    EnsCtl* ctl = (EnsCtl*)malloc(sizeof(EnsCtl) * count);
+    if (!args || !ctl) {
+        free(args);
+        free(ctl);
+        return SWE_EARG;
+    }
+    char* ws = (char*)workspace;
+    EnsCtl* ctl_dev = (EnsCtl*)(ws + ens_offset_ctl(count));
+    int rc = SWE_OK;
+    const int fric0 = members[0].params.apply_friction ? 1 + members[0].params.friction_model : 0;
+    for (int m = 0; m < count && rc == SWE_OK; ++m) {
+        const swe_ensemble_member& e = members[m];
+        StepArgs a{};
+        const int fric = e.params.apply_friction ? 1 + e.params.friction_model : 0;
+        if (fric != fric0 || !e.U_a || !e.U_b || !e.k1 || e.steps < 0 || e.rows < 1 ||
+            (e.nseries > 0 && (!e.series_t || !e.series_w)) ||
+            !fill_common(a, e.U_a, e.bed, 1, 1, e.ny, e.nx, &e.params, e.U_a, 1) ||
+            (e.params.apply_friction && !e.n)) {
+            rc = SWE_EARG;
+            break;
+        }
+        a.n = e.n;
+        a.nB = 1;
+        a.rain_mode = SWE_FORCING_NONE;
+        a.infil_mode = SWE_FORCING_NONE;
+        a.tend = e.k1;
+        a.U_out = e.U_b;
+        a.hmax = e.hmax;
+        a.max_dt = (float)e.max_dt;
+        a.rows = e.rows;
+        a.level = &ctl_dev[m].level;  // the ensemble's current level of this member
+        a.red = ctl_dev[m].red;
+        args[m] = a;
+        EnsCtl c{};
+        const int strips = (e.nx + SW_OUT - 1) / SW_OUT;
+        c.nbx = (strips + SW_WARPS - 1) / SW_WARPS;
+        c.rows = e.rows;
+        c.tiles = c.nbx * ((e.ny + e.rows - 1) / e.rows);
+        c.steps = e.steps;
+        c.nseries = e.nseries;
+        c.series_t = e.series_t;
+        c.series_w = e.series_w;
+        c.level = e.level;
+        c.start = e.start_time;
+        c.Ua = e.U_a;
+        c.Ub = e.U_b;
+        ctl[m] = c;
+    }
+    if (rc == SWE_OK) {
+        if (cudaMemcpy(ws, args, sizeof(StepArgs) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(ctl_dev, ctl, sizeof(EnsCtl) * count, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = SWE_ECUDA;
+    }
+    free(args);
+    free(ctl);
+    if (rc != SWE_OK) return rc;
+    return swe_ensemble_reset_f32(workspace, count, stream);
+}
+
+extern "C" int swe_ensemble_reset_f32(void* workspace, int count, void* stream) {
+    if (!workspace || count < 1 || count > 1024) return SWE_EARG;
+    char* ws = (char*)workspace;
+    ensemble_init_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(
+        (EnsCtl*)(ws + ens_offset_ctl(count)), count, (EnsGlobal*)(ws + ens_offset_global(count)));
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_ensemble_run_f32(void* workspace, int count, int friction, int blocks,
+                                    void* stream) {
+    if (!workspace || count < 1 || count > 1024 || blocks < 1 || friction < 0 || friction > 2)
+        return SWE_EARG;
+    char* ws = (char*)workspace;
+    const StepArgs* args = (const StepArgs*)ws;
+    EnsCtl* ctl = (EnsCtl*)(ws + ens_offset_ctl(count));
+    EnsGlobal* g = (EnsGlobal*)(ws + ens_offset_global(count));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (friction == 0) ensemble_kernel<0><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
+    else if (friction == 1) ensemble_kernel<1><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
+    else ensemble_kernel<2><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+namespace swe {
+namespace {
+__global__ void ensemble_results_kernel(const EnsCtl* ctl, int count, const EnsGlobal* g,
+                                        swe_ensemble_result* out, uint32_t* error) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) {
+        out[t].steps = ctl[t].step;
+        out[t].finished = ctl[t].finished;
+        out[t].status = ctl[t].status;
+        out[t].dt_last = ctl[t].dt_last;
+        out[t].time = ctl[t].time;
+    }
+    if (t == 0) *error = g->error;
+}
+}  // namespace
+}  // namespace swe
+
+extern "C" int swe_ensemble_results_f32(const void* workspace, int count, swe_ensemble_result* out,
+                                        uint32_t* error, void* stream) {
+    if (!workspace || !out || !error || count < 1 || count > 1024) return SWE_EARG;
+    const char* ws = (const char*)workspace;
+    ensemble_results_kernel<<<(count + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        (const EnsCtl*)(ws + ens_offset_ctl(count)), count,
+        (const EnsGlobal*)(ws + ens_offset_global(count)), out, error);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_tune_sweep_rows(int rows) {
+    if (rows < 1 || rows > 4096) return SWE_EARG;
+    g_sweep_rows = rows;
     return SWE_OK;
 }

@@ -256,8 +256,7 @@ class SWE2D(nn.Module):
         the reference.
         """
         self._check_state(U)
-        if torch.is_grad_enabled() and (U.requires_grad or (
-                torch.is_tensor(boundary_level) and boundary_level.requires_grad)):
+        if self._needs_adjoint(U, boundary_level):
             from .adjoint import step_with_adjoint
             return step_with_adjoint(self, U, model_time, max_dt, infiltration, boundary_level)
         U = nat.require_cuda_f32("U", U)
@@ -269,6 +268,14 @@ class SWE2D(nn.Module):
         U_new, status, dt = self._launch_step(U, level, max_dt_f, infiltration)
         self._raise_on_status(status, dt)
         return U_new, dt
+
+    def _needs_adjoint(self, U, boundary_level) -> bool:
+        """A step is differentiated when autograd is on and the state, the
+        boundary level or the roughness field requires grad."""
+        if not torch.is_grad_enabled():
+            return False
+        return bool(U.requires_grad or self.roughness_length.requires_grad or (
+            torch.is_tensor(boundary_level) and boundary_level.requires_grad))
 
     def _launch_step(self, U, level, max_dt_f, infiltration, red=None, scratch=None):
         """Enqueue one step; returns (U_new, status, dt) with one host read."""
@@ -361,9 +368,9 @@ class SWE2D(nn.Module):
         step: no callback, no autograd, and a positive max_dt cap if any."""
         if callback is not None or not U0.is_cuda or U0.dtype != torch.float32:
             return False
-        if torch.is_grad_enabled() and (U0.requires_grad or (
-                torch.is_tensor(boundary_level) and boundary_level.requires_grad) or (
-                boundary_level is None and self.use_dynamic_bc and self.bc_wls.requires_grad)):
+        if self._needs_adjoint(U0, boundary_level) or (
+                torch.is_grad_enabled() and boundary_level is None and self.use_dynamic_bc
+                and self.bc_wls.requires_grad):
             return False
         if max_dt_cap is not None and not self._scalar_float(max_dt_cap, "max_dt_cap") > 0.0:
             return False

@@ -168,6 +168,103 @@ int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB, 
                          int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                          float* hmax, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Adjoint of the step (the reference's autograd gradient through
+ * SWE2D.step, src/solver.py:572-663, with dt detached as in :626).
+ * --------------------------------------------------------------------- */
+
+/*
+ * Adjoint of SWE2D.spatial_operator (src/solver.py:448-531) at state S with
+ * respect to S and the boundary level: lam_S += (d rhs / d S)^T lam_rhs.
+ * scratch_cx holds B*ny*(nx+1)*12 floats, scratch_cy B*(ny+1)*nx*12.
+ * level_part receives level_blocks partial sums per batch member
+ * ([B][level_blocks]); their sum is the level adjoint of batch member b
+ * (summed over b when levelB = 1).  Deterministic (no float atomics).
+ */
+int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, int B, int ny, int nx,
+                        const swe_params* p, const float* level, int levelB,
+                        const float* lam_rhs, float* scratch_cx, float* scratch_cy, float* lam_S,
+                        float* level_part, int level_blocks, void* stream);
+
+/*
+ * Pointwise parts of the step adjoint, for step input U, tendency k and
+ * time step dt:
+ *   mode 0: corrector and friction (solver.py:646-661, friction.py:12-131):
+ *           lam_out = adjoint of the step output; lam_U += ..., lam_k = adjoint
+ *           of k2, lam_n += adjoint of the roughness field [nB,1,ny,nx];
+ *   mode 1: predictor (solver.py:639): lam_out = adjoint of P; lam_U += ...,
+ *           lam_k = adjoint of k1;
+ *   mode 2: forward predictor P_out = clean(U, U + dt/2 k) (for recompute).
+ */
+int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float* n, int nB, int B,
+                          int ny, int nx, const swe_params* p, float dt, const float* lam_out,
+                          float* lam_U, float* lam_k, float* lam_n, float* P_out, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Ensembles: many independent scenarios in one persistent launch.
+ * (No counterpart in the reference, whose batch dimension requires equal
+ * grid sizes and shares one time step, src/solver.py:367-376, :527-530.)
+ * --------------------------------------------------------------------- */
+
+/* One scenario: its own grid, bed, roughness, configuration, boundary level
+ * (constant or a series) and step count; every time step is its own CFL
+ * step (capped by max_dt).  Device pointers; the state starts in U_a and
+ * after `steps` steps is in U_a (even steps) or U_b (odd). */
+typedef struct swe_ensemble_member {
+    const float* bed;       /* [ny,nx] */
+    const float* n;         /* [ny,nx] Manning n or roughness length */
+    float* U_a;             /* [3,ny,nx] state (initial state on entry) */
+    float* U_b;             /* [3,ny,nx] second state buffer */
+    float* k1;              /* [3,ny,nx] scratch */
+    float* hmax;            /* [ny,nx] running max depth, or NULL */
+    const float* series_t;  /* boundary series times (float32), or NULL */
+    const float* series_w;  /* boundary series levels */
+    int32_t nseries;        /* 0: constant `level` */
+    int32_t ny, nx;
+    int32_t steps;          /* steps to run */
+    int32_t rows;           /* output rows per sweep tile (autotuned) */
+    float level;            /* constant boundary level when nseries == 0 */
+    double start_time;      /* absolute time of the initial state */
+    double max_dt;          /* cap on each step (float32-rounded) */
+    swe_params params;      /* all members share apply_friction / friction_model */
+} swe_ensemble_member;
+
+typedef struct swe_ensemble_result {
+    int32_t steps;     /* steps completed */
+    int32_t finished;  /* 1 done, 2 failed (status holds SWE_S_* bits) */
+    uint32_t status;
+    float dt_last;
+    double time;       /* simulated time advanced */
+} swe_ensemble_result;
+
+/* Device workspace bytes for `count` members (count <= 1024), -1 if invalid. */
+long long swe_ensemble_workspace_bytes(int count);
+
+/* Copies the members' description into `workspace` (device) and resets the
+ * ensemble's control state.  Setup only: synchronous host-to-device copies. */
+int swe_ensemble_prepare_f32(const swe_ensemble_member* members, int count, void* workspace,
+                             void* stream);
+
+/* Resets the control state (step counts, times, levels, reductions) so the
+ * ensemble can run again from its state buffers.  One small kernel. */
+int swe_ensemble_reset_f32(void* workspace, int count, void* stream);
+
+/* Runs every member for its step count in one persistent launch of `blocks`
+ * blocks of 128 threads (friction: 0 off, 1 Manning, 2 roughness length; as
+ * in the members).  Each member's stages are claimed tile by tile from
+ * per-member counters; no block waits for a particular item.  Idle polling
+ * is bounded: on the limit the kernel stops and swe_ensemble_results_f32
+ * reports error bit 1.  Capturable in a CUDA graph. */
+int swe_ensemble_run_f32(void* workspace, int count, int friction, int blocks, void* stream);
+
+/* Per-member results into out[count] (device) and the launch's error word. */
+int swe_ensemble_results_f32(const void* workspace, int count, swe_ensemble_result* out,
+                             uint32_t* error, void* stream);
+
+/* Output rows per tile of the single-grid sweep kernels (process-wide
+ * tuning knob, default 64; set it between launches, not during them). */
+int swe_tune_sweep_rows(int rows);
+
 /*
  * swe_step_noalloc_f32 -- one step like swe_step_f32, for callers that must
  * not allocate device memory.  No counterpart in the reference: it exists

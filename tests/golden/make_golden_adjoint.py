@@ -1,0 +1,146 @@
+"""Golden gradients of the reference step from PyTorch autograd (adj_*.npz).
+
+Called by make_golden.py (``--only adj``).  Every case is run twice: in
+float32 with correctly-rounded sqrt/pow (the arithmetic the kernels
+reproduce, see make_golden.py) and in float64 (the accuracy oracle).
+
+adj_step.npz  one step, random state with wet, dry and near-dry cells, for
+              several boundary / friction configurations: L = sum(w * U_new)
+              for a seeded random w; gradients w.r.t. U, the level and the
+              roughness field.
+adj_run.npz   30 steps of a 40x56 crop of the runup bathymetry across the
+              shoreline, west water level given per step (30 values), fixed
+              max_dt = 2e-3 (below the CFL step, so dt is the same in every
+              evaluation); L = sum over steps and three gauges of eta^2 plus
+              1e-3 sum(U_final^2); gradients w.r.t. U0, the 30 levels and n.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from make_golden import correctly_rounded_elementary, random_bed, random_state
+
+from diffswe2d_b200 import scenarios
+
+STEP_CASES = {
+    "walls": dict(boundary_left="wall", boundary_right="wall", boundary_top="wall",
+                  boundary_bottom="wall"),
+    "water_level": dict(boundary_left="water_level", boundary_right="water_level",
+                        boundary_top="water_level", boundary_bottom="water_level"),
+    "transmissive": dict(boundary_left="transmissive", boundary_right="transmissive",
+                         boundary_top="transmissive", boundary_bottom="transmissive"),
+    "periodic": dict(boundary_left="periodic", boundary_right="periodic", boundary_top="periodic",
+                     boundary_bottom="periodic"),
+    "mixed_a": dict(boundary_left="water_level", boundary_right="wall", boundary_top="periodic",
+                    boundary_bottom="absorbing"),
+    "mixed_b": dict(boundary_left="constant", boundary_right="transmissive", boundary_top="wall",
+                    boundary_bottom="water_level"),
+    "roughness_law": dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                          boundary_bottom="wall", frictionmodel="roughness_length"),
+    "no_friction": dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                        boundary_bottom="wall", apply_friction=False),
+    "no_reset_no_limiter": dict(boundary_left="water_level", boundary_right="wall",
+                                boundary_top="wall", boundary_bottom="wall",
+                                water_slope_reset=False, positivity_limiter=False),
+}
+
+
+def _grads_step(ref, dtype, cfg_kw, U, bed, n, level, w, dx, dy, max_dt):
+    cfg = ref.SWEConfig(**cfg_kw, constant_value=0.05)
+    m = ref.SWE2D(torch.from_numpy(bed).to(dtype), torch.from_numpy(n).to(dtype), dx, dy, config=cfg,
+                  train_dem=False)
+    m.roughness_length.requires_grad_(True)
+    Ut = torch.from_numpy(U).to(dtype).requires_grad_(True)
+    lv = torch.tensor(level, dtype=dtype, requires_grad=True)
+    Un, dt = m.step(Ut, 0.0, max_dt, boundary_level=lv)
+    loss = (Un * torch.from_numpy(w).to(dtype)).sum()
+    loss.backward()
+    gl = float(lv.grad) if lv.grad is not None else 0.0
+    gn = (m.roughness_length.grad.numpy().astype(np.float64) if m.roughness_length.grad is not None
+          else np.zeros((1, 1) + n.shape, np.float64))
+    return Ut.grad.numpy().astype(np.float64), gl, gn, dt
+
+
+def make_step_grads(ref, out):
+    rng = np.random.default_rng(77)
+    ny, nx = 11, 14
+    d = {}
+    U = random_state(rng, 1, ny, nx)
+    bed = random_bed(rng, 1, ny, nx)[0, 0]
+    n = rng.uniform(0.005, 0.04, size=(ny, nx)).astype(np.float32)
+    z0 = rng.uniform(0.0005, 0.01, size=(ny, nx)).astype(np.float32)
+    w = rng.normal(size=U.shape).astype(np.float32)
+    d["U"], d["bed"], d["n"], d["z0"], d["w"] = U, bed, n, z0, w
+    level = 0.18
+    for name, kw in STEP_CASES.items():
+        field = z0 if kw.get("frictionmodel") == "roughness_length" else n
+        with correctly_rounded_elementary():
+            gU, gl, gn, dt = _grads_step(ref, torch.float32, kw, U, bed, field, level, w, 0.05, 0.04, 0.01)
+        d[f"{name}_gU"], d[f"{name}_glevel"], d[f"{name}_gn"], d[f"{name}_dt"] = gU, gl, gn, dt
+        gU, gl, gn, dt = _grads_step(ref, torch.float64, kw, U, bed, field, level, w, 0.05, 0.04, 0.01)
+        d[f"{name}_gU64"], d[f"{name}_glevel64"], d[f"{name}_gn64"] = gU, gl, gn
+    np.savez_compressed(out / "adj_step.npz", **d)
+    print("adj_step.npz", len(STEP_CASES), "cases")
+
+
+RUN_STEPS = 30
+RUN_GAUGES = ((10, 20), (20, 30), (30, 44))
+
+
+def run_loss(ref_or_model, dtype, U0, levels, gauges, bed, n, crop_cfg, dx, steps=RUN_STEPS):
+    """Shared definition of the multi-step loss (reference side)."""
+    m = ref_or_model
+    Ut = U0
+    loss = 0.0
+    for s in range(steps):
+        Ut, _ = m.step(Ut, 0.0, 2.0e-3, boundary_level=levels[s])
+        for (iy, ix) in gauges:
+            eta = Ut[0, 0, iy, ix] + bed[iy, ix]
+            loss = loss + eta * eta
+    return loss + 1e-3 * (Ut * Ut).sum()
+
+
+def make_run_grads(ref, out):
+    sc = scenarios.runup(seed=0)
+    r0, c0 = 100, 296
+    bed = np.ascontiguousarray(sc.bed[r0:r0 + 40, c0:c0 + 56])
+    n = np.ascontiguousarray(sc.roughness[r0:r0 + 40, c0:c0 + 56])
+    U0 = np.ascontiguousarray(sc.U0[:, :, r0:r0 + 40, c0:c0 + 56])
+    dx = sc.dx
+    levels = (0.004 + 0.01 * np.sin(np.linspace(0.0, 3.0, RUN_STEPS))).astype(np.float32)
+    d = dict(bed=bed, n=n, U0=U0, levels=levels, dx=np.float64(dx),
+             gauges=np.array(RUN_GAUGES, np.int32))
+    kw = dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+              boundary_bottom="wall")
+    for dtype, tag, cr in ((torch.float32, "f32", True), (torch.float64, "f64", False)):
+        cfg = ref.SWEConfig(**kw)
+        m = ref.SWE2D(torch.from_numpy(bed).to(dtype), torch.from_numpy(n).to(dtype), dx, dx, config=cfg,
+                      train_dem=False)
+        m.roughness_length.requires_grad_(True)
+        Ut = torch.from_numpy(U0).to(dtype).requires_grad_(True)
+        lv = torch.from_numpy(levels).to(dtype).requires_grad_(True)
+        bed_t = torch.from_numpy(bed).to(dtype)
+        ctx = correctly_rounded_elementary() if cr else _Null()
+        with ctx:
+            loss = run_loss(m, dtype, Ut, lv, RUN_GAUGES, bed_t, None, None, dx)
+            loss.backward()
+        d[f"{tag}_loss"] = float(loss)
+        d[f"{tag}_gU0"] = Ut.grad.numpy().astype(np.float64)
+        d[f"{tag}_glevels"] = lv.grad.numpy().astype(np.float64)
+        d[f"{tag}_gn"] = m.roughness_length.grad.numpy().astype(np.float64)
+    np.savez_compressed(out / "adj_run.npz", **d)
+    print("adj_run.npz", d["f32_loss"], d["f64_loss"])
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def make_adjoint(ref, out):
+    make_step_grads(ref, out)
+    make_run_grads(ref, out)

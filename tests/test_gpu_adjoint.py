@@ -1,0 +1,176 @@
+"""The hand-written adjoint against the reference's autograd gradients and
+against finite differences of the FP64 oracle.
+
+Bar (north_star): adjoint gradients match the reference autograd to 1e-4
+(normwise relative, per gradient).  Fixtures: tests/golden/adj_*.npz, made by
+the reference itself (make_golden_adjoint.py) in float32 with
+correctly-rounded sqrt/pow and in float64.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import normwise
+from oracle import OracleSWE
+
+from diffswe2d_b200 import SWE2D, SWEConfig
+from diffswe2d_b200.adjoint import forward_checkpointed
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+TOL = 1e-4
+
+STEP_CASES = {
+    "walls": dict(boundary_left="wall", boundary_right="wall", boundary_top="wall",
+                  boundary_bottom="wall"),
+    "water_level": dict(boundary_left="water_level", boundary_right="water_level",
+                        boundary_top="water_level", boundary_bottom="water_level"),
+    "transmissive": dict(boundary_left="transmissive", boundary_right="transmissive",
+                         boundary_top="transmissive", boundary_bottom="transmissive"),
+    "periodic": dict(boundary_left="periodic", boundary_right="periodic", boundary_top="periodic",
+                     boundary_bottom="periodic"),
+    "mixed_a": dict(boundary_left="water_level", boundary_right="wall", boundary_top="periodic",
+                    boundary_bottom="absorbing"),
+    "mixed_b": dict(boundary_left="constant", boundary_right="transmissive", boundary_top="wall",
+                    boundary_bottom="water_level"),
+    "roughness_law": dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                          boundary_bottom="wall", frictionmodel="roughness_length"),
+    "no_friction": dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                        boundary_bottom="wall", apply_friction=False),
+    "no_reset_no_limiter": dict(boundary_left="water_level", boundary_right="wall",
+                                boundary_top="wall", boundary_bottom="wall",
+                                water_slope_reset=False, positivity_limiter=False),
+}
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("case", sorted(STEP_CASES))
+def test_one_step_vjp_matches_reference_autograd(golden, case):
+    d = golden("adj_step")
+    kw = STEP_CASES[case]
+    field = d["z0"] if kw.get("frictionmodel") == "roughness_length" else d["n"]
+    cfg = SWEConfig(**kw, constant_value=0.05)
+    m = SWE2D(_t(d["bed"]), _t(field), 0.05, 0.04, config=cfg, train_dem=False)
+    m.roughness_length.requires_grad_(True)
+    U = _t(d["U"]).requires_grad_(True)
+    lv = torch.tensor(0.18, device=DEV, requires_grad=True)
+    Un, dt = m.step(U, 0.0, 0.01, boundary_level=lv)
+    assert dt == pytest.approx(float(d[f"{case}_dt"]), rel=1e-6)
+    (Un * _t(d["w"])).sum().backward()
+    gU = U.grad.cpu().numpy()
+    eU = _rel(gU, d[f"{case}_gU"])
+    el = abs(float(lv.grad) - float(d[f"{case}_glevel"])) / max(abs(float(d[f"{case}_glevel"])), 1e-30)
+    print(case, "dL/dU", eU, "vs FP64", _rel(gU, d[f"{case}_gU64"]), "dL/dlevel", el)
+    assert eU <= TOL
+    if float(d[f"{case}_glevel"]) != 0.0:
+        assert el <= TOL
+    else:
+        assert float(lv.grad) == 0.0
+    if kw.get("apply_friction", True):
+        gn = m.roughness_length.grad.cpu().numpy()
+        assert _rel(gn, d[f"{case}_gn"]) <= TOL
+
+
+def _run_model(d, requires=True):
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall")
+    m = SWE2D(_t(d["bed"]), _t(d["n"]), float(d["dx"]), float(d["dx"]), config=cfg, train_dem=False)
+    m.roughness_length.requires_grad_(requires)
+    return m
+
+
+def _run_loss(m, U0, levels, gauges, bed):
+    U, loss = U0, 0.0
+    for s in range(levels.shape[0]):
+        U, _ = m.step(U, 0.0, 2.0e-3, boundary_level=levels[s])
+        for iy, ix in gauges:
+            eta = U[0, 0, iy, ix] + bed[iy, ix]
+            loss = loss + eta * eta
+    return loss + 1e-3 * (U * U).sum()
+
+
+def test_thirty_step_gradients_match_reference_autograd(golden):
+    d = golden("adj_run")
+    m = _run_model(d)
+    U0 = _t(d["U0"]).requires_grad_(True)
+    lv = _t(d["levels"]).requires_grad_(True)
+    loss = _run_loss(m, U0, lv, d["gauges"], _t(d["bed"]))
+    loss.backward()
+    assert float(loss) == pytest.approx(float(d["f32_loss"]), rel=1e-6)
+    errs = {
+        "U0": _rel(U0.grad.cpu().numpy(), d["f32_gU0"]),
+        "levels": _rel(lv.grad.cpu().numpy(), d["f32_glevels"]),
+        "n": _rel(m.roughness_length.grad.cpu().numpy(), d["f32_gn"]),
+    }
+    errs64 = {
+        "U0": _rel(U0.grad.cpu().numpy(), d["f64_gU0"]),
+        "levels": _rel(lv.grad.cpu().numpy(), d["f64_glevels"]),
+        "n": _rel(m.roughness_length.grad.cpu().numpy(), d["f64_gn"]),
+    }
+    print("vs reference autograd FP32", errs, "vs FP64", errs64)
+    for k, e in errs.items():
+        assert e <= TOL, k
+
+
+def test_level_gradient_matches_fp64_finite_differences(golden):
+    """Central differences (eps 1e-4) of the same loss with the FP64 oracle."""
+    d = golden("adj_run")
+    m = _run_model(d, requires=False)
+    U0 = _t(d["U0"])
+    lv = _t(d["levels"]).requires_grad_(True)
+    _run_loss(m, U0, lv, d["gauges"], _t(d["bed"])).backward()
+    g = lv.grad.cpu().numpy()
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall")
+    om = OracleSWE(d["bed"], d["n"], float(d["dx"]), float(d["dx"]), cfg, dtype=np.float64)
+
+    def loss64(levels):
+        U = d["U0"].astype(np.float64)
+        L = 0.0
+        for s in range(len(levels)):
+            U, _ = om.step(U, 0.0, 2.0e-3, boundary_level=levels[s])
+            for iy, ix in d["gauges"]:
+                L += (U[0, 0, iy, ix] + float(d["bed"][iy, ix])) ** 2
+        return L + 1e-3 * float((U * U).sum())
+
+    eps = 1e-4
+    for s in (0, 7, 15, 29):
+        up = d["levels"].astype(np.float64).copy()
+        dn = up.copy()
+        up[s] += eps
+        dn[s] -= eps
+        fd = (loss64(up) - loss64(dn)) / (2 * eps)
+        print("level", s, "adjoint", g[s], "FD64", fd)
+        assert abs(g[s] - fd) <= 1e-3 * max(abs(fd), 1e-6)
+
+
+def test_checkpointed_chunk_matches_stepwise_autograd(golden):
+    """forward_checkpointed (one autograd node per forward() call, states
+    recomputed in backward) gives the stepwise adjoint's gradients."""
+    d = golden("adj_run")
+    grads = []
+    for mode in ("chunk", "steps"):
+        m = _run_model(d)
+        U0 = _t(d["U0"]).requires_grad_(True)
+        lv = torch.tensor(0.008, device=DEV, requires_grad=True)
+        if mode == "chunk":
+            U = forward_checkpointed(m, U0, t_end=0.03, boundary_level=lv)
+        else:
+            U, _ = m(U0, t_end=0.03, boundary_level=lv, callback=lambda it, t, U: None)
+        (U[0, 0, 20, 30] ** 2 + 1e-3 * (U * U).sum()).backward()
+        grads.append((U0.grad.cpu().numpy(), float(lv.grad), m.roughness_length.grad.cpu().numpy(),
+                      U.detach().cpu().numpy()))
+    (g0c, glc, gnc, Uc), (g0s, gls, gns, Us) = grads
+    assert np.array_equal(Uc, Us)
+    assert _rel(g0c, g0s) <= 1e-6
+    assert abs(glc - gls) <= 1e-6 * max(abs(gls), 1e-30)
+    assert _rel(gnc, gns) <= 1e-6
