@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--nx", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["runup4096", "ensemble"], default="runup4096",
+                    help="runup4096: the headline single-grid step; ensemble: 64 scenarios of "
+                         "uneven sizes in one persistent launch vs 64 sequential runs")
+    ap.add_argument("--ensemble-steps", type=int, default=2000)
+    ap.add_argument("--ensemble-count", type=int, default=64)
     return ap.parse_args()
 
 
@@ -206,9 +211,98 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, world, rank, local):
+    """Config 4: scenarios with sides log-uniform in [128, 1024], each its own
+    bed, forcing, Manning n and CFL step, `--ensemble-steps` steps each, in one
+    persistent CUDA-graph-captured launch; against the same scenarios run one
+    after another with the single-grid step (two launches per step).  Under
+    torchrun each rank runs its own shard of the scenarios."""
+    from diffswe2d_b200 import scenarios
+    from diffswe2d_b200 import _native as nat
+    from diffswe2d_b200.autotune import tune
+    from diffswe2d_b200.config import SWEConfig
+    from diffswe2d_b200.ensemble import Ensemble
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sizes = scenarios.ensemble_sizes(args.ensemble_count, seed=0)
+    mine = [(k, s) for k, s in enumerate(sizes) if k % world == rank]
+    members = []
+    for k, (ny, nx) in mine:
+        sc = scenarios.ensemble_member(ny, nx, seed=k)
+        sc.steps = args.ensemble_steps
+        members.append(sc)
+    tuning = tune(dev)
+    ens = Ensemble(members, device=dev)
+    ens.run()  # warm-up (also captures the graph)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    res = ens.run()
+    ms = res.elapsed_ms
+    # sequential single-grid runs of the same scenarios
+    lib = nat.lib()
+    st = nat.stream_handle(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seq_ms = 0.0
+    from diffswe2d_b200.autotune import tuned_rows
+    for sc in members:
+        ny, nx = sc.bed.shape
+        nat.check(lib.swe_tune_sweep_rows(tuned_rows(ny * nx, dev)), "tuned rows")
+        cfg = SWEConfig(**sc.config)
+        p = nat.params(cfg, sc.dx, sc.dy)
+        bed = torch.from_numpy(sc.bed).to(dev)
+        n = torch.from_numpy(sc.roughness).to(dev)
+        U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]
+        k1 = torch.empty_like(U[0])
+        red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
+        lev = torch.full((1,), float(sc.bc_levels[0]) if sc.bc_levels is not None else 0.0, device=dev)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for s in range(sc.steps):
+            nat.check(lib.swe_step_f32(nat.ptr(U[s % 2]), nat.ptr(bed), 1, nat.ptr(n), 1, 1, ny, nx, p,
+                                       nat.ptr(lev), 1, 1.0e9, None, 0, 1, nat.ptr(k1), nat.ptr(red),
+                                       nat.ptr(U[1 - s % 2]), st), "sequential step")
+        e1.record()
+        torch.cuda.synchronize(dev)
+        seq_ms += e0.elapsed_time(e1)
+    cells = res.cell_updates
+    if world > 1:
+        t = torch.tensor([ms, seq_ms, float(cells)], device=dev, dtype=torch.float64)
+        import torch.distributed as dist
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, seq_ms, cells = float(mx[0]), float(mx[1]), int(sm[2])
+    line = {
+        "metric": "Mcell-updates/s (ensemble)", "value": cells / (ms * 1e-3) / 1e6,
+        "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.ensemble_steps, "warmup": 1,
+        "ms_per_step": ms / args.ensemble_steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"ensemble_{args.ensemble_count}_sides_128_1024",
+                   "scenarios": len(sizes), "steps_each": args.ensemble_steps,
+                   "cells_total": int(sum(a * b for a, b in sizes)),
+                   "tile_rows_by_size_class": tuning.get("rows"),
+                   "parallelism": f"scenario shards x{world}"},
+        "sequential_single_grid": {"value": cells / (seq_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+                                   "ms": seq_ms},
+        "persistent_ms": ms,
+        "gpu_launches": 2,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "ensemble" and args.impl == "b200":
+        run_ensemble(args, world, rank, local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:
@@ -226,6 +320,11 @@ def main():
     ny, nx = sc.bed.shape
     cells = ny * nx
     cfg = SWEConfig(**sc.config)
+    # launch shape from the project's autotuner (sweep tile rows per size class)
+    from diffswe2d_b200 import autotune
+    tuning = autotune.tune(dev)
+    autotune.apply(dev, cells)
+    rows_used = autotune.tuned_rows(cells, dev)
     model = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev),
                   sc.dx, sc.dy, config=cfg, train_dem=False)
     model.set_dynamic_boundary(torch.from_numpy(sc.bc_times).to(dev),
@@ -350,7 +449,8 @@ def main():
         "config": {"workload": f"runup_tiled_{ny}x{nx}", "grid": [ny, nx], "dx": sc.dx,
                    "boundaries": "west water_level (N-wave), walls", "manning": 0.01,
                    "l2": "inputs larger than L2: state 201 MB + k1 201 MB + bed/n 134 MB per replica",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}", "sweep_tile_rows": rows_used,
+                   "tuned_rows_by_size_class": tuning.get("rows")},
         "roofline": {"bound": "hbm", "kernel": "stage2 (predictor+tendency+corrector+friction)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,

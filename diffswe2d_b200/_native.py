@@ -74,6 +74,40 @@ class SweClock(ctypes.Structure):
 
 CLOCK_RUNNING, CLOCK_DONE, CLOCK_MAXSTEPS, CLOCK_FAILED = 0, 1, 2, 3
 
+
+class SweEnsembleMember(ctypes.Structure):
+    """swe_ensemble_member of include/swe_b200.h."""
+    _fields_ = [
+        ("bed", ctypes.c_void_p),
+        ("n", ctypes.c_void_p),
+        ("U_a", ctypes.c_void_p),
+        ("U_b", ctypes.c_void_p),
+        ("k1", ctypes.c_void_p),
+        ("hmax", ctypes.c_void_p),
+        ("series_t", ctypes.c_void_p),
+        ("series_w", ctypes.c_void_p),
+        ("nseries", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("nx", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("rows", ctypes.c_int32),
+        ("level", ctypes.c_float),
+        ("start_time", ctypes.c_double),
+        ("max_dt", ctypes.c_double),
+        ("params", SweParams),
+    ]
+
+
+class SweEnsembleResult(ctypes.Structure):
+    """swe_ensemble_result of include/swe_b200.h (24 bytes)."""
+    _fields_ = [
+        ("steps", ctypes.c_int32),
+        ("finished", ctypes.c_int32),
+        ("status", ctypes.c_uint32),
+        ("dt_last", ctypes.c_float),
+        ("time", ctypes.c_double),
+    ]
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -106,6 +140,12 @@ _SIGNATURES = {
     "swe_clean_and_limit_f32": [_P, _P, _I, _I, _I, ctypes.POINTER(SweParams), _P, _P],
     "swe_friction_f32": [_P, _P, _I, _I, _I, _I, _F, _I, ctypes.POINTER(SweParams), _P, _P],
     "swe_selftest_arith_f32": [_I, ctypes.c_longlong, ctypes.c_ulonglong, _P, _P, _P],
+    "swe_ensemble_prepare_f32": [ctypes.POINTER(SweEnsembleMember), _I, _P, _P],
+    "swe_ensemble_reset_f32": [_P, _I, _P],
+    "swe_ensemble_run_f32": [_P, _I, _I, _I, _P],
+    "swe_ensemble_results_f32": [_P, _I, _P, _P, _P],
+    "swe_tune_sweep_rows": [_I],
+    "swe_load_kernels": [],
 }
 
 _lib = None
@@ -124,8 +164,21 @@ def lib() -> ctypes.CDLL:
             fn = getattr(handle, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int
+        handle.swe_ensemble_workspace_bytes.argtypes = [_I]
+        handle.swe_ensemble_workspace_bytes.restype = ctypes.c_longlong
         _lib = handle
     return _lib
+
+
+_kernels_loaded = False
+
+
+def load_kernels() -> None:
+    """Load the kernels' modules once (before the first CUDA-graph capture)."""
+    global _kernels_loaded
+    if not _kernels_loaded:
+        check(lib().swe_load_kernels(), "loading kernels")
+        _kernels_loaded = True
 
 
 def exported_symbols():

@@ -1,0 +1,178 @@
+"""Autotuner for the step kernels' launch shape.
+
+Two knobs are tuned by timing them on the GPU in use:
+
+* the sweep tile height (output rows per warp strip) per grid-size class --
+  taller tiles recompute fewer halo rows, shorter ones give more tiles to
+  fill the 148 SMs on small grids; used by the single-grid kernels
+  (``swe_tune_sweep_rows``) and per scenario by ``Ensemble``;
+* the number of steps per CUDA-graph replay of ``SWE2D.forward``'s device
+  loop -- more steps per replay mean fewer host reads, more no-op steps at
+  the end of a call.
+
+Results are kept per device name in memory and in
+``$XDG_CACHE_HOME/diffswe2d_b200/autotune.json`` (default ``~/.cache``).
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from pathlib import Path
+from typing import Dict, Optional
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+SIZE_CLASSES = ((0, 1 << 16), (1 << 16, 1 << 18), (1 << 18, 1 << 20), (1 << 20, 1 << 62))
+ROW_CHOICES = (16, 32, 64, 128)
+DEFAULT_ROWS = (16, 32, 64, 64)
+CHUNK_CHOICES = (8, 16, 32, 64)
+
+_tuned: Dict[str, dict] = {}
+
+
+def _cache_file() -> Path:
+    base = os.environ.get("XDG_CACHE_HOME") or str(Path.home() / ".cache")
+    return Path(base) / "diffswe2d_b200" / "autotune.json"
+
+
+def _device_key(device) -> str:
+    props = torch.cuda.get_device_properties(torch.device(device))
+    return f"{props.name}/{props.multi_processor_count}"
+
+
+def _load(device) -> dict:
+    key = _device_key(device)
+    if key not in _tuned:
+        try:
+            _tuned[key] = json.loads(_cache_file().read_text()).get(key, {})
+        except (OSError, ValueError):
+            _tuned[key] = {}
+    return _tuned[key]
+
+
+def _store(device, entry: dict) -> None:
+    key = _device_key(device)
+    _tuned[key] = entry
+    path = _cache_file()
+    try:
+        data = json.loads(path.read_text()) if path.exists() else {}
+        data[key] = entry
+        path.parent.mkdir(parents=True, exist_ok=True)
+        path.write_text(json.dumps(data, indent=1))
+    except OSError:
+        pass
+
+
+def size_class(cells: int) -> int:
+    for k, (lo, hi) in enumerate(SIZE_CLASSES):
+        if lo <= cells < hi:
+            return k
+    return len(SIZE_CLASSES) - 1
+
+
+def tuned_rows(cells: int, device="cuda") -> int:
+    """Tile height for a grid of `cells` cells (the default if not tuned)."""
+    k = size_class(cells)
+    rows = _load(device).get("rows")
+    return int(rows[k]) if rows else DEFAULT_ROWS[k]
+
+
+def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int) -> float:
+    """ms per step of the single-grid step kernels on a runup-recipe grid."""
+    from . import scenarios
+    from .config import SWEConfig
+    sc = scenarios.tiled(scenarios.runup(seed=0), side_y, side_x)
+    dev = torch.device(device)
+    lib = nat.lib()
+    p = nat.params(SWEConfig(**sc.config), sc.dx, sc.dy)
+    bed = torch.from_numpy(sc.bed).to(dev)
+    n = torch.from_numpy(sc.roughness).to(dev)
+    U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, side_y, side_x), device=dev)]
+    k = torch.empty_like(U[0])
+    red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
+    lev = torch.full((1,), 0.005, device=dev)
+    st = nat.stream_handle(dev)
+    nat.check(lib.swe_tune_sweep_rows(rows), "tune rows")
+
+    def run(count):
+        for s in range(count):
+            rc = lib.swe_step_f32(nat.ptr(U[s % 2]), nat.ptr(bed), 1, nat.ptr(n), 1, 1, side_y, side_x,
+                                  p, nat.ptr(lev), 1, 1.0e9, None, 0, 1, nat.ptr(k), nat.ptr(red),
+                                  nat.ptr(U[1 - s % 2]), st)
+            nat.check(rc, "tune step")
+
+    run(2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(steps)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / steps
+
+
+def tune(device="cuda", steps: int = 8, force: bool = False) -> dict:
+    """Time every tile height on one representative grid per size class and
+    the graph chunk length on a small grid; store and return the choice."""
+    entry = dict(_load(device))
+    if entry.get("rows") and not force:
+        return entry
+    t0 = time.perf_counter()
+    reps = ((96, 160), (384, 512), (1024, 960), (2048, 2048))
+    rows_choice, timing = [], {}
+    for k, (ny, nx) in enumerate(reps):
+        best, best_ms = None, None
+        for r in ROW_CHOICES:
+            ms = _time_steps(ny, nx, r, device, steps)
+            timing[f"{ny}x{nx}/rows{r}"] = ms
+            if best_ms is None or ms < best_ms:
+                best, best_ms = r, ms
+        rows_choice.append(best)
+    nat.check(nat.lib().swe_tune_sweep_rows(64), "tune rows")
+    entry["rows"] = rows_choice
+    entry["chunk"] = _tune_chunk(device)
+    entry["timing_ms"] = timing
+    entry["seconds"] = time.perf_counter() - t0
+    _store(device, entry)
+    return entry
+
+
+def _tune_chunk(device) -> int:
+    from . import scenarios
+    from .config import SWEConfig
+    from .solver import SWE2D
+    sc = scenarios.runup(ny=122, nx=196, dx=0.028, seed=1)
+    dev = torch.device(device)
+    m = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev), sc.dx, sc.dy,
+              config=SWEConfig(**sc.config), train_dem=False)
+    U0 = torch.from_numpy(sc.U0).to(dev)
+    best, best_t = None, None
+    for chunk in CHUNK_CHOICES:
+        m.steps_per_chunk = chunk
+        with torch.no_grad():
+            m(U0, t_end=0.2, boundary_level=0.005)
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            m(U0, t_end=0.5, boundary_level=0.005)
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter() - t
+        if best_t is None or t < best_t:
+            best, best_t = chunk, t
+    return int(best)
+
+
+def apply(device="cuda", cells: Optional[int] = None) -> None:
+    """Use the tuned values: tile height for grids of `cells` cells (single-grid
+    kernels) and the forward() chunk length."""
+    entry = _load(device)
+    if cells is not None:
+        nat.check(nat.lib().swe_tune_sweep_rows(tuned_rows(cells, device)), "tune rows")
+    if entry.get("chunk"):
+        from .solver import SWE2D
+        SWE2D.steps_per_chunk = int(entry["chunk"])
+
+
+__all__ = ["tune", "tuned_rows", "apply", "size_class", "SIZE_CLASSES", "ROW_CHOICES", "np"]

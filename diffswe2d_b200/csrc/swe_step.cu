@@ -592,11 +592,20 @@ struct EnsCtl {
 
 struct EnsGlobal {
     unsigned int finished;  // scenarios done or failed
-    unsigned int error;     // bit 1: idle limit reached
-    unsigned int pad[14];
+    unsigned int error;     // bit 1: no progress within EnsStallNs
+    unsigned int progress;  // phases completed, all scenarios
+    unsigned int pad[13];
 };
 
-constexpr unsigned int EnsIdleLimit = 1u << 22;
+// An idle block gives up (error bit 1) only when no scenario has completed
+// a phase for this long; phases complete in microseconds to milliseconds.
+constexpr unsigned long long EnsStallNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ float ens_level(const EnsCtl& c) {
     if (c.nseries <= 0) return c.level;
@@ -628,6 +637,7 @@ __device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
             c->finished = 2;
             __threadfence();
             atomicAdd(&g->finished, 1u);
+            atomicAdd(&g->progress, 1u);
             return;
         }
     } else {  // stage 2 done: the step is complete
@@ -637,6 +647,7 @@ __device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
             c->finished = 2;
             __threadfence();
             atomicAdd(&g->finished, 1u);
+            atomicAdd(&g->progress, 1u);
             return;
         }
         c->time += (double)dt;
@@ -646,6 +657,7 @@ __device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
             c->finished = 1;
             __threadfence();
             atomicAdd(&g->finished, 1u);
+            atomicAdd(&g->progress, 1u);
             return;
         }
         c->level = ens_level(*c);
@@ -653,6 +665,7 @@ __device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
     }
     __threadfence();
     atomicExch(&c->claim, (unsigned long long)(phase + 1u) << 32);
+    atomicAdd(&g->progress, 1u);
 }
 
 template <int FRIC>
@@ -661,7 +674,8 @@ ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGl
     __shared__ StepArgs sa;
     __shared__ int s_item[3];
     int rr = (int)(blockIdx.x % (unsigned)count);
-    unsigned int idle = 0;
+    unsigned int seen_progress = 0xffffffffu, backoff = 64;
+    unsigned long long seen_at = 0;
     while (true) {
         __syncthreads();  // everyone is done with the previous item's shared data
         if (threadIdx.x == 0) {
@@ -680,17 +694,24 @@ ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGl
                 }
             }
             if (item == -2) {
+                const unsigned int prog = *(volatile unsigned int*)&g->progress;
+                const unsigned long long now = global_ns();
                 if (*(volatile unsigned int*)&g->finished >= (unsigned int)count ||
                     *(volatile unsigned int*)&g->error) {
                     item = -1;
-                } else if (++idle > EnsIdleLimit) {
+                } else if (prog != seen_progress) {
+                    seen_progress = prog;
+                    seen_at = now;
+                    __nanosleep(backoff);
+                } else if (now - seen_at > EnsStallNs) {
                     atomicOr(&g->error, 1u);
                     item = -1;
                 } else {
-                    __nanosleep(256);
+                    __nanosleep(backoff);
+                    backoff = min(backoff * 2u, 4096u);
                 }
             } else {
-                idle = 0;
+                backoff = 64;
                 __threadfence();
             }
             s_item[0] = item;
@@ -736,6 +757,7 @@ __global__ void ensemble_init_kernel(EnsCtl* ctl, int count, EnsGlobal* g) {
     if (t == 0) {
         g->finished = 0u;
         g->error = 0u;
+        g->progress = 0u;
     }
     __syncthreads();
     if (t < count) {
@@ -1117,5 +1139,22 @@ extern "C" int swe_ensemble_results_f32(const void* workspace, int count, swe_en
 extern "C" int swe_tune_sweep_rows(int rows) {
     if (rows < 1 || rows > 4096) return SWE_EARG;
     g_sweep_rows = rows;
+    return SWE_OK;
+}
+
+extern "C" int swe_load_kernels(void) {
+    // Touching each kernel loads its module now (CUDA lazy loading), so that
+    // no first load happens inside a stream capture.
+    cudaFuncAttributes at;
+    const void* fns[] = {
+        (const void*)stage_kernel<1>,        (const void*)stage_kernel<2>,
+        (const void*)sweep_kernel<1, 0>,     (const void*)sweep_kernel<2, 0>,
+        (const void*)sweep_kernel<2, 1>,     (const void*)sweep_kernel<2, 2>,
+        (const void*)ensemble_kernel<0>,     (const void*)ensemble_kernel<1>,
+        (const void*)ensemble_kernel<2>,     (const void*)ensemble_init_kernel,
+        (const void*)ensemble_results_kernel,
+    };
+    for (const void* f : fns)
+        if (cudaFuncGetAttributes(&at, f) != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }

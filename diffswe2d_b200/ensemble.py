@@ -1,0 +1,160 @@
+"""Ensembles of independent scenarios in one persistent, CUDA-graph-captured launch.
+
+The reference batches scenarios through its batch dimension, which needs equal
+grid sizes and shares one time step across the batch (``src/solver.py:367-376``,
+``:527-530``).  ``Ensemble`` runs scenarios of different grid sizes, each with
+its own configuration, roughness, boundary series, CFL time step and step
+count, in one launch of the persistent kernel of ``csrc/swe_step.cu``
+(``swe_ensemble_run_f32``); the launch (with its control-state reset) is
+captured in a CUDA graph and replayed.  Each scenario's result is bit for bit
+what ``SWE2D.step`` gives for that scenario alone.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import torch
+
+from . import _native as nat
+from .config import SWEConfig
+
+
+@dataclass
+class EnsembleResult:
+    states: List[torch.Tensor]   # final [1,3,ny,nx] state of each scenario
+    steps: List[int]
+    times: List[float]           # simulated time advanced
+    hmax: Optional[List[torch.Tensor]]
+    elapsed_ms: float            # device time of the persistent launch
+    cell_updates: int
+
+    @property
+    def mcells_per_s(self) -> float:
+        return self.cell_updates / (self.elapsed_ms * 1e-3) / 1e6
+
+
+class Ensemble:
+    """Scenarios (``diffswe2d_b200.scenarios.Scenario`` or compatible) on one GPU.
+
+    ``rows`` fixes the sweep tile height of every scenario; by default it is
+    chosen per grid-size class by ``autotune.tuned_rows``.
+    """
+
+    def __init__(self, scenarios: Sequence, device="cuda", steps: Optional[int] = None,
+                 rows: Optional[int] = None, track_hmax: bool = False, max_dt: float = 1.0e9):
+        from .autotune import tuned_rows
+        self.device = torch.device(device)
+        self.count = len(scenarios)
+        if not 1 <= self.count <= 1024:
+            raise ValueError("an ensemble holds 1 to 1024 scenarios")
+        self._keep = []  # tensors referenced by the device member table
+        members = (nat.SweEnsembleMember * self.count)()
+        fric = None
+        self.cells = []
+        self.steps = []
+        self.U_a, self.U_b, self.hmax = [], [], []
+        for m, sc in enumerate(scenarios):
+            cfg = SWEConfig(**sc.config)
+            f = (1 + (0 if cfg.frictionmodel == "manning" else 1)) if cfg.apply_friction else 0
+            if fric is None:
+                fric = f
+            elif f != fric:
+                raise ValueError("all scenarios of an ensemble must use the same friction law")
+            ny, nx = sc.bed.shape
+            dev = self.device
+            bed = torch.as_tensor(sc.bed, dtype=torch.float32, device=dev).contiguous()
+            n = torch.as_tensor(sc.roughness, dtype=torch.float32, device=dev).contiguous()
+            Ua = torch.as_tensor(sc.U0, dtype=torch.float32, device=dev).reshape(3, ny, nx).clone()
+            Ub = torch.empty_like(Ua)
+            k1 = torch.empty_like(Ua)
+            hm = Ua[0].clone() if track_hmax else None
+            st = sw = None
+            nser = 0
+            if sc.bc_times is not None:
+                st = torch.as_tensor(sc.bc_times, dtype=torch.float32, device=dev).contiguous()
+                sw = torch.as_tensor(sc.bc_levels, dtype=torch.float32, device=dev).contiguous()
+                nser = st.numel()
+            steps_m = int(sc.steps if steps is None else steps)
+            r = int(rows) if rows is not None else tuned_rows(ny * nx, dev)
+            mem = members[m]
+            mem.bed, mem.n = bed.data_ptr(), n.data_ptr()
+            mem.U_a, mem.U_b, mem.k1 = Ua.data_ptr(), Ub.data_ptr(), k1.data_ptr()
+            mem.hmax = hm.data_ptr() if hm is not None else None
+            mem.series_t = st.data_ptr() if st is not None else None
+            mem.series_w = sw.data_ptr() if sw is not None else None
+            mem.nseries, mem.ny, mem.nx, mem.steps, mem.rows = nser, ny, nx, steps_m, r
+            mem.level = float(cfg.constant_level)
+            mem.start_time = 0.0
+            mem.max_dt = float(max_dt)
+            mem.params = nat.params(cfg, sc.dx, sc.dy)
+            self._keep += [bed, n, Ua, Ub, k1, hm, st, sw]
+            self.U_a.append(Ua)
+            self.U_b.append(Ub)
+            self.hmax.append(hm)
+            self.cells.append(ny * nx)
+            self.steps.append(steps_m)
+        self.friction = fric
+        self.initial = [u.clone() for u in self.U_a]
+        lib = nat.lib()
+        nbytes = lib.swe_ensemble_workspace_bytes(self.count)
+        if nbytes < 0:
+            raise ValueError("invalid ensemble size")
+        self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+        self.results_dev = torch.empty(self.count * ctypes.sizeof(nat.SweEnsembleResult),
+                                       dtype=torch.uint8, device=self.device)
+        self.error_dev = torch.zeros(1, dtype=torch.int32, device=self.device)
+        rc = lib.swe_ensemble_prepare_f32(members, self.count, nat.ptr(self.workspace),
+                                          nat.stream_handle(self.device))
+        nat.check(rc, "ensemble prepare")
+        props = torch.cuda.get_device_properties(self.device)
+        self.blocks = props.multi_processor_count * 6
+        self._graph = None
+
+    def _launch(self):
+        lib, st = nat.lib(), nat.stream_handle(self.device)
+        nat.check(lib.swe_ensemble_reset_f32(nat.ptr(self.workspace), self.count, st), "ensemble reset")
+        nat.check(lib.swe_ensemble_run_f32(nat.ptr(self.workspace), self.count, self.friction,
+                                           self.blocks, st), "ensemble run")
+
+    def run(self) -> EnsembleResult:
+        """Run every scenario from its initial state; returns final states."""
+        for Ua, U0 in zip(self.U_a, self.initial):
+            Ua.copy_(U0)
+        for hm, U0 in zip(self.hmax, self.initial):
+            if hm is not None:
+                hm.copy_(U0[0])
+        if self._graph is None:
+            nat.load_kernels()
+            self._graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self._graph):
+                self._launch()
+            for Ua, U0 in zip(self.U_a, self.initial):  # capture ran nothing; keep inputs
+                Ua.copy_(U0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        self._graph.replay()
+        e1.record()
+        lib = nat.lib()
+        nat.check(lib.swe_ensemble_results_f32(nat.ptr(self.workspace), self.count,
+                                               nat.ptr(self.results_dev), nat.ptr(self.error_dev),
+                                               nat.stream_handle(self.device)), "ensemble results")
+        torch.cuda.synchronize(self.device)
+        raw = bytes(self.results_dev.cpu().numpy())
+        res = (nat.SweEnsembleResult * self.count).from_buffer_copy(raw)
+        if int(self.error_dev.item()) != 0:
+            raise RuntimeError("ensemble kernel stopped: idle limit reached")
+        states, steps, times = [], [], []
+        for m in range(self.count):
+            r = res[m]
+            if r.finished == 2:
+                raise FloatingPointError(f"scenario {m}: time step failed (status {r.status})")
+            buf = self.U_a[m] if r.steps % 2 == 0 else self.U_b[m]
+            states.append(buf.clone().unsqueeze(0))
+            steps.append(int(r.steps))
+            times.append(float(r.time))
+        hmax = [h.clone() if h is not None else None for h in self.hmax] if any(
+            h is not None for h in self.hmax) else None
+        total = sum(c * s for c, s in zip(self.cells, steps))
+        return EnsembleResult(states, steps, times, hmax, e0.elapsed_time(e1), total)

@@ -380,100 +380,72 @@ class SWE2D(nn.Module):
                         boundary_level, max_dt_cap):
         """forward() with the time loop on the device (src/solver.py:680-779).
 
-        Each chunk of ``steps_per_chunk`` steps is one CUDA-graph replay of
-        [stage 1, stage 2, clock] launches; the host reads the 72-byte clock
-        once per chunk.  Results are those of the host loop bit for bit.
+        Each chunk of ``steps_per_chunk`` steps is one replay of a CUDA graph
+        of [stage 1, stage 2, clock] launches; the host reads the 72-byte
+        clock once per chunk.  The graph and its buffers are captured once per
+        shape and configuration (``_DeviceLoop``) and reused by later calls.
+        Results are those of the host loop bit for bit.
         """
         self._check_state(U0)
         U0 = nat.require_cuda_f32("U0", U0.detach())
         dev = U0.device
         B, _, ny, nx = U0.shape
         bed, n = self._fields(U0)
-        series_t = series_w = None
-        nseries = 0
         if boundary_level is not None:
             lv, levelB = self._level_arg(self._prepare_boundary_level(boundary_level, U0), B)
+            series = None
         elif self.use_dynamic_bc:
-            series_t = self.bc_times.detach().to(dtype=torch.float32, device=dev).contiguous()
-            series_w = self.bc_wls.detach().to(dtype=torch.float32, device=dev).contiguous()
-            nseries = series_t.numel()
-            lv, levelB = torch.zeros(1, dtype=torch.float32, device=dev), 1
+            lv, levelB = None, 1
+            series = (self.bc_times.detach().to(dtype=torch.float32, device=dev),
+                      self.bc_wls.detach().to(dtype=torch.float32, device=dev))
         else:
             lv, levelB = self._level_arg(self._prepare_boundary_level(self.cfg.constant_level, U0), B)
+            series = None
         infil, imode, iB = self._forcing_arg(infiltration, U0[:, 0:1])
-        bufs = [U0.clone(), torch.empty_like(U0)]
-        scratch = torch.empty_like(U0)
-        red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
-        hmax = U0[:, 0].clone()
-        cap = self._scalar_float(max_dt_cap, "max_dt_cap") if max_dt_cap is not None else 0.0
-        clock_host = nat.SweClock(duration, absolute_start, max(1e-12, 1e-12 * abs(duration)),
-                                  cap, 0.0, max_steps, 0, 0, 0, 0, 0.0, 0.0, 0.0)
-        clock = torch.frombuffer(bytearray(bytes(clock_host)), dtype=torch.uint8).to(dev)
         names = list(self.gauge_indices) if self.track_gauges else []
-        chunk = self.steps_per_chunk
-        cells = gbuf = None
-        if names:
-            idx = [self.gauge_indices[name] for name in names]
-            for iy, ix in idx:
-                if not (0 <= iy < ny and 0 <= ix < nx):
-                    raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
-            cells = torch.tensor(idx, dtype=torch.int32, device=dev).reshape(-1).contiguous()
-            gbuf = torch.zeros((chunk, 2 + len(names)), dtype=torch.float64, device=dev)
-        lib, p = nat.lib(), self._params()
-
-        def clock_tick(state):
-            rc = lib.swe_clock_f32(nat.ptr(clock), nat.ptr(red), nat.ptr(series_t), nat.ptr(series_w),
-                                   nseries, nat.ptr(lv), nat.ptr(state), ny, nx, nat.ptr(cells),
-                                   len(names), nat.ptr(gbuf), chunk if names else 0,
-                                   nat.stream_handle(dev))
-            nat.check(rc, "forward clock")
-
-        def one_step(src, dst):
-            rc = lib.swe_step_clocked_f32(3, nat.ptr(src), nat.ptr(bed), bed.shape[0], nat.ptr(n),
-                                          n.shape[0], B, ny, nx, p, nat.ptr(lv), levelB,
-                                          nat.ptr(clock), nat.ptr(infil), imode, iB,
-                                          nat.ptr(scratch), nat.ptr(red), nat.ptr(dst),
-                                          nat.ptr(hmax), nat.stream_handle(dev))
-            nat.check(rc, "forward step")
-            clock_tick(dst)
-
-        clock_tick(bufs[0])  # sets up the first step
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            for s in range(chunk):
-                one_step(bufs[s % 2], bufs[1 - s % 2])
-        bed_at = None
+        cells = []
+        for name in names:
+            iy, ix = self.gauge_indices[name]
+            if not (0 <= iy < ny and 0 <= ix < nx):
+                raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
+            cells.append((int(iy), int(ix)))
+        p = self._params()
+        key = (B, ny, nx, str(dev), bed.shape[0], n.shape[0], levelB,
+               None if series is None else series[0].numel(), tuple(cells), imode, iB,
+               None if infil is None else tuple(infil.shape), self.steps_per_chunk, bytes(p))
+        loops = self.__dict__.setdefault("_device_loops", {})
+        loop = loops.get(key)
+        if loop is None:
+            loop = _DeviceLoop(self, key, B, ny, nx, dev, bed.shape, n.shape, levelB, series, cells,
+                               infil, imode, iB, p, self.steps_per_chunk)
+            loops[key] = loop
+        cap = self._scalar_float(max_dt_cap, "max_dt_cap") if max_dt_cap is not None else 0.0
+        clock = nat.SweClock(duration, absolute_start, max(1e-12, 1e-12 * abs(duration)), cap, 0.0,
+                             max_steps, 0, 0, 0, 0, 0.0, 0.0, 0.0)
+        steps_seen = 0
+        bed_at = {}
         if names:
             bed0 = self.bed.detach()[0, 0]
-            bed_at = {name: float(bed0[iy, ix]) for name, (iy, ix) in zip(names, idx)}
-        steps_seen = 0
-        try:
-            while True:
-                graph.replay()
-                raw = clock.cpu().numpy().tobytes()
-                c = nat.SweClock.from_buffer_copy(raw)
-                if names and c.steps > steps_seen:
-                    rows = gbuf.cpu().numpy()
-                    for s in range(steps_seen, c.steps):
-                        r = rows[s % chunk]
-                        self.ts_time.append(float(r[0]))
-                        self.ts_dt.append(float(r[1]))
-                        for g, name in enumerate(names):
-                            depth = float(r[2 + g])
-                            self.ts_h.setdefault(name, []).append(depth)
-                            self.ts_z.setdefault(name, []).append(depth + bed_at[name])
-                steps_seen = c.steps
-                if c.state == nat.CLOCK_FAILED:
-                    self._raise_on_status(c.dt_status, float(c.last_dt))
-                if c.state == nat.CLOCK_DONE:
-                    break
-                if c.state == nat.CLOCK_MAXSTEPS:
-                    raise RuntimeError(f"max_steps={max_steps} reached after {c.elapsed:.8f} s; "
-                                       f"requested duration={duration:.8f} s.")
-        finally:
-            del graph
+            bed_at = {name: float(bed0[iy, ix]) for name, (iy, ix) in zip(names, cells)}
+        for state, c in loop.run(U0, bed, n, lv, series, infil, clock):
+            if names and c.steps > steps_seen:
+                rows = loop.gbuf.cpu().numpy()
+                for k in range(steps_seen, c.steps):
+                    r = rows[k % loop.chunk]
+                    self.ts_time.append(float(r[0]))
+                    self.ts_dt.append(float(r[1]))
+                    for g, name in enumerate(names):
+                        depth = float(r[2 + g])
+                        self.ts_h.setdefault(name, []).append(depth)
+                        self.ts_z.setdefault(name, []).append(depth + bed_at[name])
+            steps_seen = c.steps
+            if c.state == nat.CLOCK_FAILED:
+                self._raise_on_status(c.dt_status, float(c.last_dt))
+            if c.state == nat.CLOCK_MAXSTEPS:
+                raise RuntimeError(f"max_steps={max_steps} reached after {c.elapsed:.8f} s; "
+                                   f"requested duration={duration:.8f} s.")
         self.last_forward_steps = steps_seen
-        return bufs[0], hmax
+        return loop.bufs[0].clone(), loop.hmax.clone()
 
     def _record_gauges(self, U: torch.Tensor, absolute_time: float, dt_value: float) -> None:
         """Micro-step gauge records (src/solver.py:781-801)."""
@@ -487,3 +459,82 @@ class SWE2D(nn.Module):
             bed = float(current_bed[0, 0, iy, ix].detach().cpu())
             self.ts_h[name].append(depth)
             self.ts_z[name].append(depth + bed)
+
+
+class _DeviceLoop:
+    """Buffers and captured CUDA graph of the device-driven forward() loop for
+    one (shape, configuration) of a model.  Inputs are copied into the
+    buffers at each call; the graph runs ``chunk`` steps per replay."""
+
+    def __init__(self, model, key, B, ny, nx, dev, bed_shape, n_shape, levelB, series, cells, infil,
+                 imode, iB, params, chunk):
+        self.chunk = int(chunk)
+        self.bufs = [torch.empty((B, 3, ny, nx), device=dev), torch.empty((B, 3, ny, nx), device=dev)]
+        self.scratch = torch.empty((B, 3, ny, nx), device=dev)
+        self.red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+        self.hmax = torch.empty((B, ny, nx), device=dev)
+        self.bed = torch.empty(bed_shape, device=dev)
+        self.n = torch.empty(n_shape, device=dev)
+        self.lv = torch.zeros(levelB, device=dev)
+        self.nseries = 0 if series is None else series[0].numel()
+        self.series_t = None if series is None else torch.empty(self.nseries, device=dev)
+        self.series_w = None if series is None else torch.empty(self.nseries, device=dev)
+        self.infil = None if infil is None else torch.empty_like(infil)
+        self.imode, self.iB = imode, iB
+        self.ncells = len(cells)
+        self.cells = (torch.tensor(cells, dtype=torch.int32, device=dev).reshape(-1).contiguous()
+                      if cells else None)
+        self.gbuf = (torch.zeros((self.chunk, 2 + self.ncells), dtype=torch.float64, device=dev)
+                     if cells else None)
+        self.clock = torch.zeros(72, dtype=torch.uint8, device=dev)
+        self.clock_host = torch.zeros(72, dtype=torch.uint8).pin_memory()
+        self.params = params
+        self.B, self.ny, self.nx, self.levelB, self.dev = B, ny, nx, levelB, dev
+        self.graph = None
+
+    def _clock_tick(self, state):
+        rc = nat.lib().swe_clock_f32(
+            nat.ptr(self.clock), nat.ptr(self.red), nat.ptr(self.series_t), nat.ptr(self.series_w),
+            self.nseries, nat.ptr(self.lv), nat.ptr(state), self.ny, self.nx, nat.ptr(self.cells),
+            self.ncells, nat.ptr(self.gbuf), self.chunk if self.ncells else 0,
+            nat.stream_handle(self.dev))
+        nat.check(rc, "forward clock")
+
+    def _step(self, src, dst):
+        rc = nat.lib().swe_step_clocked_f32(
+            3, nat.ptr(src), nat.ptr(self.bed), self.bed.shape[0], nat.ptr(self.n), self.n.shape[0],
+            self.B, self.ny, self.nx, self.params, nat.ptr(self.lv), self.levelB,
+            nat.ptr(self.clock), nat.ptr(self.infil), self.imode, self.iB, nat.ptr(self.scratch),
+            nat.ptr(self.red), nat.ptr(dst), nat.ptr(self.hmax), nat.stream_handle(self.dev))
+        nat.check(rc, "forward step")
+        self._clock_tick(dst)
+
+    def run(self, U0, bed, n, lv, series, infil, clock):
+        """Yields (state buffer, clock) after each replay until the call ends."""
+        self.bufs[0].copy_(U0)
+        self.hmax.copy_(U0[:, 0])
+        self.bed.copy_(bed)
+        self.n.copy_(n)
+        if lv is not None:
+            self.lv.copy_(lv.reshape(-1))
+        if series is not None:
+            self.series_t.copy_(series[0])
+            self.series_w.copy_(series[1])
+        if infil is not None:
+            self.infil.copy_(infil)
+        self.clock_host.copy_(torch.frombuffer(bytearray(bytes(clock)), dtype=torch.uint8))
+        self.clock.copy_(self.clock_host, non_blocking=True)
+        self._clock_tick(self.bufs[0])  # sets up the first step
+        if self.graph is None:
+            nat.load_kernels()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                for s in range(self.chunk):
+                    self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
+            self.graph = graph
+        while True:
+            self.graph.replay()
+            c = nat.SweClock.from_buffer_copy(self.clock.cpu().numpy().tobytes())
+            yield self.bufs[0], c
+            if c.state != nat.CLOCK_RUNNING:
+                return

@@ -253,13 +253,18 @@ int swe_ensemble_reset_f32(void* workspace, int count, void* stream);
  * blocks of 128 threads (friction: 0 off, 1 Manning, 2 roughness length; as
  * in the members).  Each member's stages are claimed tile by tile from
  * per-member counters; no block waits for a particular item.  Idle polling
- * is bounded: on the limit the kernel stops and swe_ensemble_results_f32
- * reports error bit 1.  Capturable in a CUDA graph. */
+ * backs off and is bounded: if no member completes a phase for 2 s the
+ * blocks stop and swe_ensemble_results_f32 reports error bit 1.  Capturable
+ * in a CUDA graph. */
 int swe_ensemble_run_f32(void* workspace, int count, int friction, int blocks, void* stream);
 
 /* Per-member results into out[count] (device) and the launch's error word. */
 int swe_ensemble_results_f32(const void* workspace, int count, swe_ensemble_result* out,
                              uint32_t* error, void* stream);
+
+/* Loads every step/ensemble kernel's module now (CUDA loads kernels lazily
+ * on first launch); call once before capturing launches in a CUDA graph. */
+int swe_load_kernels(void);
 
 /* Output rows per tile of the single-grid sweep kernels (process-wide
  * tuning knob, default 64; set it between launches, not during them). */
