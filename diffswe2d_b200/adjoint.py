@@ -34,12 +34,30 @@ def _check_no_bed_grad(model):
             "the B200 adjoint; construct the model with train_dem=False")
 
 
-def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None):
+class AdjointWorkspace:
+    """Scratch buffers of adjoint_step for one state shape (reused across steps)."""
+
+    def __init__(self, B, ny, nx, dev):
+        shape = (B, 3, ny, nx)
+        self.K1, self.K2, self.P = (torch.empty(shape, device=dev) for _ in range(3))
+        self.lam_k = torch.empty(shape, device=dev)
+        self.lam_P = torch.empty(shape, device=dev)
+        self.red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
+        self.cx = torch.empty(B * ny * (nx + 1) * 12, device=dev)
+        self.cy = torch.empty(B * (ny + 1) * nx * 12, device=dev)
+        self.part = torch.empty(B * LEVEL_BLOCKS, device=dev)
+        self.key = (B, ny, nx, str(dev))
+
+
+def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None, ws=None, lam_U=None,
+                 lam_n=None):
     """VJP of one step at input state ``U`` with time step ``dt``.
 
     Returns ``(lam_U, lam_level, lam_n)``: adjoints of the state
     [B,3,ny,nx], the level vector (1 or B values) and the roughness field
-    (same shape as ``n``; None when friction is off).
+    (same shape as ``n``; None when friction is off).  ``ws`` is an optional
+    AdjointWorkspace; ``lam_U`` / ``lam_n`` optional zeroed outputs that the
+    step accumulates into.
     """
     U = nat.require_cuda_f32("U", U.detach())
     lam_out = nat.require_cuda_f32("lam_out", lam_out)
@@ -51,8 +69,9 @@ def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None):
     infil, imode, iB = model._forcing_arg(infiltration, U[:, 0:1])
     p = model._params()
     lib, st = nat.lib(), nat.stream_handle(dev)
-    K1, K2, P = torch.empty_like(U), torch.empty_like(U), torch.empty_like(U)
-    red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
+    if ws is None or ws.key != (B, ny, nx, str(dev)):
+        ws = AdjointWorkspace(B, ny, nx, dev)
+    K1, K2, P, red = ws.K1, ws.K2, ws.P, ws.red
 
     def tendency(S, out):
         rc = lib.swe_spatial_operator_f32(nat.ptr(S), nat.ptr(bed), B, bed.shape[0], ny, nx, p,
@@ -66,14 +85,14 @@ def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None):
                                    None, None, None, None, nat.ptr(P), st)
     nat.check(rc, "adjoint predictor")
     tendency(P, K2)
-    lam_U = torch.zeros_like(U)
-    lam_k = torch.empty_like(U)
-    lam_P = torch.zeros_like(U)
+    lam_U = torch.zeros_like(U) if lam_U is None else lam_U
+    lam_k = ws.lam_k
+    lam_P = ws.lam_P
+    lam_P.zero_()
     fric = bool(model.cfg.apply_friction)
-    lam_n = torch.zeros_like(n) if fric else None
-    cx = torch.empty(B * ny * (nx + 1) * 12, dtype=torch.float32, device=dev)
-    cy = torch.empty(B * (ny + 1) * nx * 12, dtype=torch.float32, device=dev)
-    part = torch.empty(B * LEVEL_BLOCKS, dtype=torch.float32, device=dev)
+    if fric and lam_n is None:
+        lam_n = torch.zeros_like(n)
+    cx, cy, part = ws.cx, ws.cy, ws.part
     # corrector + friction
     rc = lib.swe_adj_pointwise_f32(0, nat.ptr(U), nat.ptr(K2), nat.ptr(n), n.shape[0], B, ny, nx, p,
                                    float(dt), nat.ptr(lam_out), nat.ptr(lam_U), nat.ptr(lam_k),
@@ -145,8 +164,10 @@ class _ChunkFunction(torch.autograd.Function):
             U, _ = model.forward(U0.detach(), t_end=t_end, start_time=start_time,
                                  boundary_level=level_vec.detach(), max_dt_cap=max_dt_cap,
                                  max_steps=max_steps)
-        steps_out.append(getattr(model, "last_forward_steps", None))
+        steps = getattr(model, "last_forward_steps", None)
+        steps_out.append(steps)
         ctx.model, ctx.t_end, ctx.max_dt_cap, ctx.max_steps = model, t_end, max_dt_cap, max_steps
+        ctx.start_time, ctx.steps = start_time, steps
         ctx.save_for_backward(U0, level_vec, n)
         return U
 
@@ -154,36 +175,60 @@ class _ChunkFunction(torch.autograd.Function):
     def backward(ctx, gU):
         U0, level_vec, n = ctx.saved_tensors
         model = ctx.model
-        # recompute the chunk's states with the reference's loop (solver.py:738-768)
-        duration = float(ctx.t_end)
-        tolerance = max(1e-12, 1e-12 * abs(duration))
-        states, dts, elapsed, U = [], [], 0.0, U0.detach()
-        with torch.no_grad():
-            for _ in range(ctx.max_steps):
-                remaining = duration - elapsed
-                if remaining <= tolerance:
-                    break
-                step_max = remaining if ctx.max_dt_cap is None else min(remaining, float(ctx.max_dt_cap))
-                max_dt_f = float(torch.tensor(step_max, dtype=torch.float32).item())
-                U_new, status, dt = model._launch_step(U, level_vec.detach(), max_dt_f, None)
-                model._raise_on_status(status, dt)
-                states.append(U)
-                dts.append(dt)
-                U = U_new
-                elapsed += dt
-                if elapsed > duration and elapsed - duration <= tolerance:
-                    elapsed = duration
+        states, dts = _recompute_chunk(model, U0.detach(), level_vec.detach(), float(ctx.t_end),
+                                       float(ctx.start_time), ctx.max_dt_cap, ctx.steps)
         lam = gU.contiguous()
         lam_level = torch.zeros_like(level_vec)
         lam_n = torch.zeros_like(n) if model.cfg.apply_friction else None
+        B, _, ny, nx = U0.shape
+        ws = AdjointWorkspace(B, ny, nx, U0.device)
         for U_s, dt_s in zip(reversed(states), reversed(dts)):
-            lam, l_lev, l_n = adjoint_step(model, U_s, level_vec, n, dt_s, lam)
+            lam, l_lev, lam_n = adjoint_step(model, U_s, level_vec, n, dt_s, lam, ws=ws, lam_n=lam_n)
             lam_level += l_lev.reshape(lam_level.shape)
-            if lam_n is not None:
-                lam_n += l_n
         g_level = lam_level if ctx.needs_input_grad[1] else None
         g_n = lam_n if (ctx.needs_input_grad[2] and lam_n is not None) else None
         return lam, g_level, g_n, None, None, None, None, None, None
+
+
+def _recompute_chunk(model, U0, level_vec, duration, start_time, max_dt_cap, steps):
+    """States entering each step of one forward() call and their time steps,
+    recomputed with the device clock (same kernels and bookkeeping as the
+    forward pass, so the same states bit for bit) and one host read."""
+    dev = U0.device
+    B, _, ny, nx = U0.shape
+    bed, n = model._fields(U0)
+    lv, levelB = model._level_arg(level_vec, B)
+    p = model._params()
+    lib, st = nat.lib(), nat.stream_handle(dev)
+    cap = float(max_dt_cap) if max_dt_cap is not None else 0.0
+    clock_host = nat.SweClock(duration, start_time, max(1e-12, 1e-12 * abs(duration)), cap, 0.0,
+                              int(steps), 0, 0, 0, 0, 0.0, 0.0, 0.0)
+    clock = torch.frombuffer(bytearray(bytes(clock_host)), dtype=torch.uint8).to(dev)
+    red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+    scratch = torch.empty_like(U0)
+    rec = torch.zeros((max(int(steps), 1), 2), dtype=torch.float64, device=dev)
+
+    def tick(state):
+        rc = lib.swe_clock_f32(nat.ptr(clock), nat.ptr(red), None, None, 0, nat.ptr(lv), nat.ptr(state),
+                               ny, nx, None, 0, nat.ptr(rec), int(steps), st)
+        nat.check(rc, "recompute clock")
+
+    tick(U0)
+    states = [U0]
+    for _ in range(int(steps)):
+        out = torch.empty_like(U0)
+        rc = lib.swe_step_clocked_f32(3, nat.ptr(states[-1]), nat.ptr(bed), bed.shape[0], nat.ptr(n),
+                                      n.shape[0], B, ny, nx, p, nat.ptr(lv), levelB, nat.ptr(clock),
+                                      None, nat.FORCING_NONE, 1, nat.ptr(scratch), nat.ptr(red),
+                                      nat.ptr(out), None, st)
+        nat.check(rc, "recompute step")
+        tick(out)
+        states.append(out)
+    c = nat.SweClock.from_buffer_copy(clock.cpu().numpy().tobytes())
+    if c.state == nat.CLOCK_FAILED:
+        model._raise_on_status(c.dt_status, float(c.last_dt))
+    dts = [float(x) for x in rec[:, 1].cpu().tolist()][: c.steps]
+    return states[: c.steps], dts
 
 
 def forward_checkpointed(model, U0, t_end, start_time=0.0, boundary_level=None, max_dt_cap=None,

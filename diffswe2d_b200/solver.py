@@ -339,6 +339,7 @@ class SWE2D(nn.Module):
         for iteration in range(max_steps):
             remaining = duration - elapsed
             if remaining <= tolerance:
+                self.last_forward_steps = iteration
                 return U, hmax
             step_max_dt = remaining
             if max_dt_cap is not None:

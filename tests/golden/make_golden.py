@@ -17,7 +17,9 @@ Fixtures (numpy .npz, float32 unless noted):
                   1/10/100/1000 and the FP64 reference (rounded to float32)
   c2_runup.npz    244x393 runup config with dynamic west water level,
                   FP32 states at steps 1/50/200 and a forward() chunk
-  adj_small.npz   reference autograd gradients through a short run
+  adj_step.npz, adj_run.npz   reference autograd gradients (make_golden_adjoint.py)
+  spline.npz      clamped B-spline basis and bounded controls of the
+                  reference's inversion script
 """
 from __future__ import annotations
 
@@ -296,6 +298,33 @@ def main():
     if "adj" in groups:
         from make_golden_adjoint import make_adjoint  # noqa: E402
         make_adjoint(ref, HERE)
+    if "spline" in groups:
+        make_spline(args.ref, HERE)
+
+
+
+def make_spline(ref_root, out):
+    """Clamped cubic B-spline basis of the reference's inversion script
+    (Examples/inverse/**/bc_inversion_train.py:189-231) for two sample grids."""
+    import importlib.util
+    import pathlib as _pl
+    script = next(_pl.Path(ref_root).glob("Examples/inverse/*/*_6simg/bc_inversion_train.py"))
+    spec = importlib.util.spec_from_file_location("bc_inversion_train", script)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    d = {}
+    for tag, (t_end, n, ctl) in {"a": (22.5, 1125, 16), "b": (29.8, 150, 20), "c": (22.5, 226, 16)}.items():
+        times = torch.linspace(0.0, t_end, n, dtype=torch.float64)
+        basis, knots, greville = mod.build_clamped_bspline_basis(times, ctl, 3)
+        d[f"{tag}_times"] = times.numpy()
+        d[f"{tag}_basis"] = basis.numpy()
+        d[f"{tag}_knots"] = knots.numpy()
+        d[f"{tag}_greville"] = greville.numpy()
+        raw = torch.linspace(-2.0, 2.0, ctl, dtype=torch.float64)
+        d[f"{tag}_raw"] = raw.numpy()
+        d[f"{tag}_bounded"] = mod.bounded_control_values(raw).numpy()
+    np.savez_compressed(out / "spline.npz", **d)
+    print("spline.npz", len(d))
 
 
 if __name__ == "__main__":

@@ -8,11 +8,16 @@ adj_step.npz  one step, random state with wet, dry and near-dry cells, for
               several boundary / friction configurations: L = sum(w * U_new)
               for a seeded random w; gradients w.r.t. U, the level and the
               roughness field.
-adj_run.npz   30 steps of a 40x56 crop of the runup bathymetry across the
-              shoreline, west water level given per step (30 values), fixed
-              max_dt = 2e-3 (below the CFL step, so dt is the same in every
-              evaluation); L = sum over steps and three gauges of eta^2 plus
-              1e-3 sum(U_final^2); gradients w.r.t. U0, the 30 levels and n.
+adj_run.npz   30 steps of a 40x56 crop of the runup bathymetry above the
+              shoreline (dry at the start, flooded from the west), west water
+              level given per step (30 values), fixed max_dt = 2e-3 (below the
+              CFL step, so dt is the same in every evaluation); L = sum over
+              steps and three gauges of eta^2 plus 1e-3 sum(U_final^2);
+              gradients w.r.t. U0, the 30 levels and n.
+adj_run_wet.npz  the same on a crop across the shoreline (92 % wet at the
+              start), where U0 and n have smooth gradients for finite
+              differences (every U0 entry of the dry crop sits on the wet/dry
+              kink).
 """
 from __future__ import annotations
 
@@ -101,9 +106,8 @@ def run_loss(ref_or_model, dtype, U0, levels, gauges, bed, n, crop_cfg, dx, step
     return loss + 1e-3 * (Ut * Ut).sum()
 
 
-def make_run_grads(ref, out):
+def make_run_grads(ref, out, name="adj_run", r0=100, c0=296):
     sc = scenarios.runup(seed=0)
-    r0, c0 = 100, 296
     bed = np.ascontiguousarray(sc.bed[r0:r0 + 40, c0:c0 + 56])
     n = np.ascontiguousarray(sc.roughness[r0:r0 + 40, c0:c0 + 56])
     U0 = np.ascontiguousarray(sc.U0[:, :, r0:r0 + 40, c0:c0 + 56])
@@ -129,8 +133,8 @@ def make_run_grads(ref, out):
         d[f"{tag}_gU0"] = Ut.grad.numpy().astype(np.float64)
         d[f"{tag}_glevels"] = lv.grad.numpy().astype(np.float64)
         d[f"{tag}_gn"] = m.roughness_length.grad.numpy().astype(np.float64)
-    np.savez_compressed(out / "adj_run.npz", **d)
-    print("adj_run.npz", d["f32_loss"], d["f64_loss"])
+    np.savez_compressed(out / f"{name}.npz", **d)
+    print(f"{name}.npz", d["f32_loss"], d["f64_loss"])
 
 
 class _Null:
@@ -144,3 +148,4 @@ class _Null:
 def make_adjoint(ref, out):
     make_step_grads(ref, out)
     make_run_grads(ref, out)
+    make_run_grads(ref, out, "adj_run_wet", 100, 170)

@@ -98,14 +98,15 @@ def _run_loss(m, U0, levels, gauges, bed):
     return loss + 1e-3 * (U * U).sum()
 
 
-def test_thirty_step_gradients_match_reference_autograd(golden):
-    d = golden("adj_run")
+@pytest.mark.parametrize("fixture", ["adj_run", "adj_run_wet"])
+def test_thirty_step_gradients_match_reference_autograd(golden, fixture):
+    d = golden(fixture)
     m = _run_model(d)
     U0 = _t(d["U0"]).requires_grad_(True)
     lv = _t(d["levels"]).requires_grad_(True)
     loss = _run_loss(m, U0, lv, d["gauges"], _t(d["bed"]))
     loss.backward()
-    assert float(loss) == pytest.approx(float(d["f32_loss"]), rel=1e-6)
+    assert float(loss.detach()) == pytest.approx(float(d["f32_loss"]), rel=1e-6)
     errs = {
         "U0": _rel(U0.grad.cpu().numpy(), d["f32_gU0"]),
         "levels": _rel(lv.grad.cpu().numpy(), d["f32_glevels"]),
@@ -158,8 +159,14 @@ def test_level_gradient_matches_fp64_finite_differences(golden):
 
 
 def test_state_and_roughness_gradients_match_fp64_finite_differences(golden):
-    """Central differences of the 30-step loss w.r.t. entries of U0 and n."""
-    d = golden("adj_run")
+    """Central differences of the 30-step loss w.r.t. entries of U0 and n, on
+    the crop across the shoreline (adj_run_wet).  Momentum entries and n are
+    smooth at the FD scale (eps 1e-7 absolute for U0, 1e-4 relative for n;
+    bar 1e-3).  Depth entries sit on a piecewise-smooth surface -- the
+    minmod/limiter branches of 30 steps switch inside any usable eps, and the
+    reference's own FP32 and FP64 autograd gradients differ by about 1 % there
+    -- so they get a 2 % bar."""
+    d = golden("adj_run_wet")
     m = _run_model(d)
     U0 = _t(d["U0"]).requires_grad_(True)
     lv = _t(d["levels"])
@@ -179,20 +186,26 @@ def test_state_and_roughness_gradients_match_fp64_finite_differences(golden):
         return L + 1e-3 * float((U * U).sum())
 
     n64 = d["n"].astype(np.float64)
-    for idx in np.argsort(-np.abs(gU).ravel())[:3]:
-        e = 1e-4 * max(1.0, abs(float(d["U0"].ravel()[idx])))
-        up, dn = d["U0"].astype(np.float64).ravel().copy(), d["U0"].astype(np.float64).ravel().copy()
+    U064 = d["U0"].astype(np.float64)
+    cells = U064.shape[2] * U064.shape[3]
+    wet = U064[0, 0].ravel() > 5e-3
+    order = np.argsort(-np.abs(gU).ravel())
+    momentum = [i for i in order if i >= cells and wet[i % cells]][:3]
+    depth = [i for i in order if i < cells and wet[i]][:3]
+    for idx, bar in [(i, 1e-3) for i in momentum] + [(i, 2e-2) for i in depth]:
+        e = 1e-7
+        up, dn = U064.ravel().copy(), U064.ravel().copy()
         up[idx] += e
         dn[idx] -= e
-        fd = (loss64(up.reshape(d["U0"].shape), n64) - loss64(dn.reshape(d["U0"].shape), n64)) / (2 * e)
+        fd = (loss64(up.reshape(U064.shape), n64) - loss64(dn.reshape(U064.shape), n64)) / (2 * e)
         print("U0", idx, gU.ravel()[idx], fd)
-        assert abs(gU.ravel()[idx] - fd) <= 1e-3 * abs(fd)
+        assert abs(gU.ravel()[idx] - fd) <= bar * abs(fd)
     for idx in np.argsort(-np.abs(gn).ravel())[:2]:
         e = 1e-4 * float(d["n"].ravel()[idx])
         up, dn = n64.ravel().copy(), n64.ravel().copy()
         up[idx] += e
         dn[idx] -= e
-        fd = (loss64(d["U0"], up.reshape(n64.shape)) - loss64(d["U0"], dn.reshape(n64.shape))) / (2 * e)
+        fd = (loss64(U064, up.reshape(n64.shape)) - loss64(U064, dn.reshape(n64.shape))) / (2 * e)
         print("n", idx, gn.ravel()[idx], fd)
         assert abs(gn.ravel()[idx] - fd) <= 1e-3 * abs(fd)
 

@@ -121,3 +121,25 @@ def test_oracle_step_errors():
     U[0, 1, 3, 3] = np.nan
     with pytest.raises(FloatingPointError, match="non-finite"):
         m.step(U, 0.0, 1.0)
+
+
+@pytest.mark.parametrize("fixture", ["adj_run", "adj_run_wet"])
+def test_thirty_step_loss_matches_reference(golden, fixture):
+    """The 30-step loss of the adjoint fixtures: the FP64 oracle against the
+    reference's FP64 run, the FP32 oracle against its FP32 run with
+    correctly-rounded sqrt/pow (the finite-difference checks of the adjoint
+    differentiate this oracle loss)."""
+    d = golden(fixture)
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall")
+    for dtype, key, rel in ((np.float64, "f64_loss", 1e-12), (np.float32, "f32_loss", 1e-6)):
+        om = OracleSWE(d["bed"], d["n"], float(d["dx"]), float(d["dx"]), cfg, dtype=dtype)
+        U = d["U0"].astype(dtype)
+        L = dtype(0.0)
+        for s in range(len(d["levels"])):
+            U, _ = om.step(U, 0.0, 2.0e-3, boundary_level=dtype(d["levels"][s]))
+            for iy, ix in d["gauges"]:
+                eta = U[0, 0, iy, ix] + dtype(d["bed"][iy, ix])
+                L = L + eta * eta
+        L = L + dtype(1e-3) * (U * U).sum(dtype=dtype)
+        assert float(L) == pytest.approx(float(d[key]), rel=rel)
