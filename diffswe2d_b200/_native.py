@@ -14,7 +14,7 @@ import torch
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libswe_b200.so"
 
 SWE_OK, SWE_EARG, SWE_ECUDA = 0, 1, 2
-S_NONFINITE_STATE, S_NONFINITE_DT, S_NONPOSITIVE_DT = 1, 2, 4
+S_NONFINITE_STATE, S_NONFINITE_DT, S_NONPOSITIVE_DT, S_STEP_LIMIT = 1, 2, 4, 8
 RED_WORDS = 8
 FORCING_NONE, FORCING_SCALAR, FORCING_FIELD = 0, 1, 2
 
@@ -72,7 +72,21 @@ class SweClock(ctypes.Structure):
     ]
 
 
-CLOCK_RUNNING, CLOCK_DONE, CLOCK_MAXSTEPS, CLOCK_FAILED = 0, 1, 2, 3
+CLOCK_RUNNING, CLOCK_DONE, CLOCK_MAXSTEPS, CLOCK_FAILED, CLOCK_RECORD_FULL = 0, 1, 2, 3, 4
+
+
+class SweRunClock(ctypes.Structure):
+    """swe_run_clock of include/swe_b200.h (104 bytes)."""
+    _fields_ = [
+        ("base", SweClock),
+        ("out_dt", ctypes.c_double),
+        ("n_out", ctypes.c_int32),
+        ("chunk", ctypes.c_int32),
+        ("chunk_steps", ctypes.c_int32),
+        ("record_cap", ctypes.c_int32),
+        ("replay", ctypes.c_int32),
+        ("replay_end", ctypes.c_int32),
+    ]
 
 
 class SweEnsembleMember(ctypes.Structure):
@@ -95,6 +109,12 @@ class SweEnsembleMember(ctypes.Structure):
         ("start_time", ctypes.c_double),
         ("max_dt", ctypes.c_double),
         ("params", SweParams),
+        ("out_dt", ctypes.c_double),
+        ("n_out", ctypes.c_int32),
+        ("ngauge", ctypes.c_int32),
+        ("out_levels", ctypes.c_void_p),
+        ("gauge_cells", ctypes.c_void_p),
+        ("gauge_out", ctypes.c_void_p),
     ]
 
 
@@ -121,12 +141,19 @@ _SIGNATURES = {
     "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                            _F, _P, _I, _I, _P, _P, _P, _P],
     "swe_clock_f32": [_P, _P, _P, _P, _I, _P, _P, _I, _I, _P, _I, _P, _I, _P],
+    "swe_run_clock_f32": [_P, _P, _P, _I, _P, _P, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _P],
+    "swe_gauge_adjoint_f32": [_P, _I, _I, _I, _P, _I, _P, _I, _I, _P],
     "swe_step_clocked_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _P, _P, _I, _I, _P, _P, _P, _P, _P],
     "swe_adj_spatial_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _P, _P,
                             _P, _P, _I, _P],
     "swe_adj_pointwise_f32": [_I, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _F, _P,
                               _P, _P, _P, _P, _P],
+    "swe_adj_pointwise_dev_f32": [_I, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P,
+                                  _P, _P, _P, _P, _P, _P],
+    "swe_gauge_adjoint_prep_f32": [_P, _P, _P, _P, _I, _P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _I,
+                                   _P],
+    "swe_gauge_adjoint_post_f32": [_P, _P, _P, _I, _I, _I, _I, _P, _I, _P],
     "swe_step_noalloc_f32": [_P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _F, _P, _I, _I, _P, _P, _P],
     "swe_ghost_cells_f32": [_P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _I,
@@ -145,7 +172,18 @@ _SIGNATURES = {
     "swe_ensemble_run_f32": [_P, _I, _I, _I, _P],
     "swe_ensemble_results_f32": [_P, _I, _P, _P, _P],
     "swe_tune_sweep_rows": [_I],
+    "swe_sweep_rows": [],
     "swe_load_kernels": [],
+    # include/nn_b200.h
+    "nn_gemm_bf16": [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P],
+    "nn_im2col": [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _F, _P, _I, _P],
+    "nn_col2im": [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P],
+    "nn_act_backward": [_P, _P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _P],
+    "nn_colsum": [_P, _I, _I, _I, _P, _P],
+    "nn_transpose_bf16": [_P, _I, _I, _I, _P, _I, _P],
+    "nn_cast_bf16": [_P, _I, _I, _I, _P, _I, _P, _I, _P],
+    "nn_mse": [_P, _P, _I, _I, _P, _P, _P],
+    "nn_adam": [_P, _P, _P, _P, ctypes.c_longlong, _F, _F, _F, _F, _I, _P],
 }
 
 _lib = None

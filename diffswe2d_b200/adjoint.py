@@ -34,19 +34,95 @@ def _check_no_bed_grad(model):
             "the B200 adjoint; construct the model with train_dem=False")
 
 
-class AdjointWorkspace:
-    """Scratch buffers of adjoint_step for one state shape (reused across steps)."""
+class AdjointStepper:
+    """The step adjoint's kernels for one model, state shape and level form,
+    with their scratch buffers allocated once (a run's backward pass calls
+    it once per step)."""
 
-    def __init__(self, B, ny, nx, dev):
+    def __init__(self, model, B, ny, nx, dev, levelB, infiltration=None):
         shape = (B, 3, ny, nx)
+        self.model = model
+        self.B, self.ny, self.nx, self.levelB = B, ny, nx, levelB
         self.K1, self.K2, self.P = (torch.empty(shape, device=dev) for _ in range(3))
         self.lam_k = torch.empty(shape, device=dev)
         self.lam_P = torch.empty(shape, device=dev)
         self.red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
         self.cx = torch.empty(B * ny * (nx + 1) * 12, device=dev)
         self.cy = torch.empty(B * (ny + 1) * nx * 12, device=dev)
-        self.part = torch.empty(B * LEVEL_BLOCKS, device=dev)
-        self.key = (B, ny, nx, str(dev))
+        self.part = torch.empty((2, B * LEVEL_BLOCKS), device=dev)
+        probe = torch.empty((B, 1, ny, nx), device=dev)
+        self.bed, self.n = model._fields(probe.expand(B, 3, ny, nx))
+        self.infil, self.imode, self.iB = model._forcing_arg(infiltration, probe)
+        self.p = model._params()
+        self.fric = bool(model.cfg.apply_friction)
+        self.lib, self.dev = nat.lib(), dev
+        self.key = (B, ny, nx, str(dev), levelB)
+
+    @property
+    def st(self):
+        # the current stream at each call, so launches inside a CUDA-graph
+        # capture land in the graph
+        return nat.stream_handle(self.dev)
+
+    def _tendency(self, S, lv, out):
+        rc = self.lib.swe_spatial_operator_f32(
+            nat.ptr(S), nat.ptr(self.bed), self.B, self.bed.shape[0], self.ny, self.nx, self.p,
+            nat.ptr(lv), self.levelB, None, nat.FORCING_NONE, 1, nat.ptr(self.infil), self.imode,
+            self.iB, nat.ptr(out), nat.ptr(self.red), self.st)
+        nat.check(rc, "adjoint recompute")
+
+    def _pointwise(self, mode, U, k, dt, lam_out, lam_U, lam_n, P_out):
+        n = self.n
+        nptr = nat.ptr(n) if mode == 0 else None
+        lnptr = nat.ptr(lam_n) if (mode == 0 and self.fric) else None
+        if torch.is_tensor(dt):  # device time step (graph-captured backward passes)
+            rc = self.lib.swe_adj_pointwise_dev_f32(
+                mode, nat.ptr(U), nat.ptr(k), nptr, n.shape[0], self.B, self.ny, self.nx, self.p,
+                nat.ptr(dt), nat.ptr(lam_out), nat.ptr(lam_U), nat.ptr(self.lam_k), lnptr,
+                nat.ptr(P_out), self.st)
+        else:
+            rc = self.lib.swe_adj_pointwise_f32(
+                mode, nat.ptr(U), nat.ptr(k), nptr, n.shape[0], self.B, self.ny, self.nx, self.p,
+                float(dt), nat.ptr(lam_out), nat.ptr(lam_U), nat.ptr(self.lam_k), lnptr,
+                nat.ptr(P_out), self.st)
+        nat.check(rc, ("adjoint corrector", "adjoint predictor", "adjoint predictor")[mode])
+
+    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n):
+        """lam_U += (d U_new / d U)^T lam_out and lam_n += the roughness
+        adjoint (when friction is on) for the step at input state U with
+        level vector lv and time step dt (a float, or a one-element device
+        tensor); returns the level adjoint's partial sums
+        [2, B * LEVEL_BLOCKS] (their sum per batch member is that member's
+        level adjoint)."""
+        lib, st, p, B, ny, nx = self.lib, self.st, self.p, self.B, self.ny, self.nx
+        K1, K2, P, lam_k, lam_P = self.K1, self.K2, self.P, self.lam_k, self.lam_P
+        # recompute the step's stage intermediates (solver.py:613-646)
+        self._tendency(U, lv, K1)
+        self._pointwise(2, U, K1, dt, None, None, None, P)
+        self._tendency(P, lv, K2)
+        lam_P.zero_()
+        # corrector + friction
+        self._pointwise(0, U, K2, dt, lam_out, lam_U, lam_n, None)
+        # spatial operator at the predictor
+        rc = lib.swe_adj_spatial_f32(nat.ptr(P), nat.ptr(self.bed), self.bed.shape[0], B, ny, nx, p,
+                                     nat.ptr(lv), self.levelB, nat.ptr(lam_k), nat.ptr(self.cx),
+                                     nat.ptr(self.cy), nat.ptr(lam_P), nat.ptr(self.part[0]),
+                                     LEVEL_BLOCKS, st)
+        nat.check(rc, "adjoint spatial operator (stage 2)")
+        # predictor
+        self._pointwise(1, U, K1, dt, lam_P, lam_U, None, None)
+        # spatial operator at the input state
+        rc = lib.swe_adj_spatial_f32(nat.ptr(U), nat.ptr(self.bed), self.bed.shape[0], B, ny, nx, p,
+                                     nat.ptr(lv), self.levelB, nat.ptr(lam_k), nat.ptr(self.cx),
+                                     nat.ptr(self.cy), nat.ptr(lam_U), nat.ptr(self.part[1]),
+                                     LEVEL_BLOCKS, st)
+        nat.check(rc, "adjoint spatial operator (stage 1)")
+        return self.part
+
+    def level_adjoint(self, part):
+        """Level adjoint [levelB] from the partial sums of one step."""
+        lam = part.view(2, self.B, LEVEL_BLOCKS).sum(dim=(0, 2))
+        return lam.sum(0, keepdim=True) if self.levelB == 1 else lam
 
 
 def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None, ws=None, lam_U=None,
@@ -56,67 +132,21 @@ def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None, ws=None, la
     Returns ``(lam_U, lam_level, lam_n)``: adjoints of the state
     [B,3,ny,nx], the level vector (1 or B values) and the roughness field
     (same shape as ``n``; None when friction is off).  ``ws`` is an optional
-    AdjointWorkspace; ``lam_U`` / ``lam_n`` optional zeroed outputs that the
-    step accumulates into.
+    AdjointStepper built for the same model and shapes; ``lam_U`` / ``lam_n``
+    optional zeroed outputs that the step accumulates into.
     """
     U = nat.require_cuda_f32("U", U.detach())
     lam_out = nat.require_cuda_f32("lam_out", lam_out)
     B, _, ny, nx = U.shape
     dev = U.device
-    bed, _ = model._fields(U)
-    n = nat.require_cuda_f32("n", n.detach())
     lv, levelB = model._level_arg(level.detach(), B)
-    infil, imode, iB = model._forcing_arg(infiltration, U[:, 0:1])
-    p = model._params()
-    lib, st = nat.lib(), nat.stream_handle(dev)
-    if ws is None or ws.key != (B, ny, nx, str(dev)):
-        ws = AdjointWorkspace(B, ny, nx, dev)
-    K1, K2, P, red = ws.K1, ws.K2, ws.P, ws.red
-
-    def tendency(S, out):
-        rc = lib.swe_spatial_operator_f32(nat.ptr(S), nat.ptr(bed), B, bed.shape[0], ny, nx, p,
-                                          nat.ptr(lv), levelB, None, nat.FORCING_NONE, 1,
-                                          nat.ptr(infil), imode, iB, nat.ptr(out), nat.ptr(red), st)
-        nat.check(rc, "adjoint recompute")
-
-    # recompute the step's stage intermediates (solver.py:613-646)
-    tendency(U, K1)
-    rc = lib.swe_adj_pointwise_f32(2, nat.ptr(U), nat.ptr(K1), None, 1, B, ny, nx, p, float(dt),
-                                   None, None, None, None, nat.ptr(P), st)
-    nat.check(rc, "adjoint predictor")
-    tendency(P, K2)
+    if ws is None or ws.key != (B, ny, nx, str(dev), levelB):
+        ws = AdjointStepper(model, B, ny, nx, dev, levelB, infiltration)
     lam_U = torch.zeros_like(U) if lam_U is None else lam_U
-    lam_k = ws.lam_k
-    lam_P = ws.lam_P
-    lam_P.zero_()
-    fric = bool(model.cfg.apply_friction)
-    if fric and lam_n is None:
-        lam_n = torch.zeros_like(n)
-    cx, cy, part = ws.cx, ws.cy, ws.part
-    # corrector + friction
-    rc = lib.swe_adj_pointwise_f32(0, nat.ptr(U), nat.ptr(K2), nat.ptr(n), n.shape[0], B, ny, nx, p,
-                                   float(dt), nat.ptr(lam_out), nat.ptr(lam_U), nat.ptr(lam_k),
-                                   nat.ptr(lam_n), None, st)
-    nat.check(rc, "adjoint corrector")
-    # spatial operator at the predictor
-    rc = lib.swe_adj_spatial_f32(nat.ptr(P), nat.ptr(bed), bed.shape[0], B, ny, nx, p, nat.ptr(lv),
-                                 levelB, nat.ptr(lam_k), nat.ptr(cx), nat.ptr(cy), nat.ptr(lam_P),
-                                 nat.ptr(part), LEVEL_BLOCKS, st)
-    nat.check(rc, "adjoint spatial operator (stage 2)")
-    lam_level = part.view(B, LEVEL_BLOCKS).sum(1)
-    # predictor
-    rc = lib.swe_adj_pointwise_f32(1, nat.ptr(U), nat.ptr(K1), None, 1, B, ny, nx, p, float(dt),
-                                   nat.ptr(lam_P), nat.ptr(lam_U), nat.ptr(lam_k), None, None, st)
-    nat.check(rc, "adjoint predictor")
-    # spatial operator at the input state
-    rc = lib.swe_adj_spatial_f32(nat.ptr(U), nat.ptr(bed), bed.shape[0], B, ny, nx, p, nat.ptr(lv),
-                                 levelB, nat.ptr(lam_k), nat.ptr(cx), nat.ptr(cy), nat.ptr(lam_U),
-                                 nat.ptr(part), LEVEL_BLOCKS, st)
-    nat.check(rc, "adjoint spatial operator (stage 1)")
-    lam_level = lam_level + part.view(B, LEVEL_BLOCKS).sum(1)
-    if levelB == 1:
-        lam_level = lam_level.sum(0, keepdim=True)
-    return lam_U, lam_level, lam_n
+    if ws.fric and lam_n is None:
+        lam_n = torch.zeros_like(ws.n)
+    part = ws(U, lv, dt, lam_out, lam_U, lam_n)
+    return lam_U, ws.level_adjoint(part), (lam_n if ws.fric else None)
 
 
 class _StepFunction(torch.autograd.Function):
@@ -181,7 +211,7 @@ class _ChunkFunction(torch.autograd.Function):
         lam_level = torch.zeros_like(level_vec)
         lam_n = torch.zeros_like(n) if model.cfg.apply_friction else None
         B, _, ny, nx = U0.shape
-        ws = AdjointWorkspace(B, ny, nx, U0.device)
+        ws = AdjointStepper(model, B, ny, nx, U0.device, model._level_arg(level_vec, B)[1])
         for U_s, dt_s in zip(reversed(states), reversed(dts)):
             lam, l_lev, lam_n = adjoint_step(model, U_s, level_vec, n, dt_s, lam, ws=ws, lam_n=lam_n)
             lam_level += l_lev.reshape(lam_level.shape)

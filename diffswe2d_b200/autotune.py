@@ -4,8 +4,10 @@ Two knobs are tuned by timing them on the GPU in use:
 
 * the sweep tile height (output rows per warp strip) per grid-size class --
   taller tiles recompute fewer halo rows, shorter ones give more tiles to
-  fill the 148 SMs on small grids; used by the single-grid kernels
-  (``swe_tune_sweep_rows``) and per scenario by ``Ensemble``;
+  fill the 148 SMs on small grids and a shorter serial chain per warp; used
+  by the single-grid kernels (``swe_tune_sweep_rows``) and per scenario by
+  ``Ensemble``; and per exact (batch, ny, nx) shape for the captured time
+  loops of gauge runs and ``SWE2D.forward`` (``tuned_rows_for_shape``);
 * the number of steps per CUDA-graph replay of ``SWE2D.forward``'s device
   loop -- more steps per replay mean fewer host reads, more no-op steps at
   the end of a call.
@@ -27,7 +29,7 @@ import torch
 from . import _native as nat
 
 SIZE_CLASSES = ((0, 1 << 16), (1 << 16, 1 << 18), (1 << 18, 1 << 20), (1 << 20, 1 << 62))
-ROW_CHOICES = (16, 32, 64, 128)
+ROW_CHOICES = (4, 8, 16, 32, 64, 128)
 DEFAULT_ROWS = (16, 32, 64, 64)
 CHUNK_CHOICES = (8, 16, 32, 64)
 
@@ -81,8 +83,9 @@ def tuned_rows(cells: int, device="cuda") -> int:
     return int(rows[k]) if rows else DEFAULT_ROWS[k]
 
 
-def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int) -> float:
-    """ms per step of the single-grid step kernels on a runup-recipe grid."""
+def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int, batch: int = 1) -> float:
+    """ms per step of the single-grid step kernels on a runup-recipe grid
+    (``batch`` copies of it)."""
     from . import scenarios
     from .config import SWEConfig
     sc = scenarios.tiled(scenarios.runup(seed=0), side_y, side_x)
@@ -91,7 +94,8 @@ def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int) -> floa
     p = nat.params(SWEConfig(**sc.config), sc.dx, sc.dy)
     bed = torch.from_numpy(sc.bed).to(dev)
     n = torch.from_numpy(sc.roughness).to(dev)
-    U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, side_y, side_x), device=dev)]
+    U0 = torch.from_numpy(sc.U0).to(dev).expand(batch, 3, side_y, side_x).contiguous()
+    U = [U0, torch.empty_like(U0)]
     k = torch.empty_like(U[0])
     red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
     lev = torch.full((1,), 0.005, device=dev)
@@ -100,7 +104,7 @@ def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int) -> floa
 
     def run(count):
         for s in range(count):
-            rc = lib.swe_step_f32(nat.ptr(U[s % 2]), nat.ptr(bed), 1, nat.ptr(n), 1, 1, side_y, side_x,
+            rc = lib.swe_step_f32(nat.ptr(U[s % 2]), nat.ptr(bed), 1, nat.ptr(n), 1, batch, side_y, side_x,
                                   p, nat.ptr(lev), 1, 1.0e9, None, 0, 1, nat.ptr(k), nat.ptr(red),
                                   nat.ptr(U[1 - s % 2]), st)
             nat.check(rc, "tune step")
@@ -164,6 +168,47 @@ def _tune_chunk(device) -> int:
     return int(best)
 
 
+def tuned_rows_for_shape(batch: int, ny: int, nx: int, device="cuda", steps: int = 6) -> int:
+    """Tile height for a time loop over [batch, 3, ny, nx] states: timed on
+    that shape (runup recipe) the first time it is asked for, then cached."""
+    entry = _load(device)
+    key = f"{batch}x{ny}x{nx}"
+    shapes = entry.setdefault("shapes", {})
+    if key in shapes:
+        return int(shapes[key])
+    prev = int(nat.lib().swe_sweep_rows())
+    best, best_ms = None, None
+    try:
+        for r in ROW_CHOICES:
+            if r > 2 * ny and best is not None:
+                break
+            ms = _time_steps(ny, nx, r, device, steps, batch)
+            if best_ms is None or ms < best_ms:
+                best, best_ms = r, ms
+    finally:
+        nat.check(nat.lib().swe_tune_sweep_rows(prev), "tune rows")
+    shapes[key] = int(best)
+    _store(device, entry)
+    return int(best)
+
+
+class sweep_rows:
+    """Context manager: the single-grid kernels use ``rows`` inside (e.g.
+    while a CUDA graph is captured), the previous value after."""
+
+    def __init__(self, rows: int):
+        self.rows = int(rows)
+
+    def __enter__(self):
+        self.prev = int(nat.lib().swe_sweep_rows())
+        nat.check(nat.lib().swe_tune_sweep_rows(self.rows), "tune rows")
+        return self
+
+    def __exit__(self, *exc):
+        nat.check(nat.lib().swe_tune_sweep_rows(self.prev), "tune rows")
+        return False
+
+
 def apply(device="cuda", cells: Optional[int] = None) -> None:
     """Use the tuned values: tile height for grids of `cells` cells (single-grid
     kernels) and the forward() chunk length."""
@@ -175,4 +220,5 @@ def apply(device="cuda", cells: Optional[int] = None) -> None:
         SWE2D.steps_per_chunk = int(entry["chunk"])
 
 
-__all__ = ["tune", "tuned_rows", "apply", "size_class", "SIZE_CLASSES", "ROW_CHOICES", "np"]
+__all__ = ["tune", "tuned_rows", "tuned_rows_for_shape", "sweep_rows", "apply", "size_class",
+           "SIZE_CLASSES", "ROW_CHOICES", "np"]

@@ -310,6 +310,7 @@ struct PwArgs {
     float* P;           // mode 2: predictor output
     float scale;        // dt (mode 0) or dt/2 (modes 1, 2)
     float dt;
+    const float* dt_dev;  // if set: dt read from device memory (scale derived here)
     int B, nB, ny, nx, mode, positivity, friction, friction_model;
     SweConsts kc;
 };
@@ -370,7 +371,7 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
     const bool moving = wet && sp2 > 0.0f;
     const float S = fmaxf(sp2, k.fr_e2);
     const float speed = moving ? sqrtf(S) : 0.0f;
-    float cf, l_h_cf = 0.0f, l_n_cf = 0.0f;
+    float cf;
     // cf and d cf / d h, d cf / d n (as autograd evaluates them)
     float dcf_dpre = 0.0f, dcf_dn = 0.0f, hpre = 0.0f;
     bool h_pass = false, n_pass = false;
@@ -439,23 +440,26 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
     float l_h = 0.0f;
     if (h >= k.fr_vs) l_h += l_safe;
     if (h_pass) l_h += l_cf * dcf_dpre;
-    l_h_cf = l_h;
-    (void)l_n_cf;
     ln = n_pass ? l_cf * dcf_dn : 0.0f;
-    if (s0.h >= 0.0f) ls.h += l_h_cf;
+    if (s0.h >= 0.0f) ls.h += l_h;
 }
 
 __global__ void adj_pointwise_kernel(const PwArgs a) {
     const long long plane = (long long)a.ny * a.nx;
     const long long total = plane * a.B;
+    float dt = a.dt, scale = a.scale;
+    if (a.dt_dev != nullptr) {
+        dt = *a.dt_dev;
+        scale = a.mode == 0 ? dt : 0.5f * dt;
+    }
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(t / plane);
         const long long i = t - (long long)b * plane;
         const size_t o = (size_t)b * 3 * plane + i;
         const State u{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
-        const State cand{u.h + a.scale * a.k[o], u.hu + a.scale * a.k[o + plane],
-                         u.hv + a.scale * a.k[o + 2 * plane]};
+        const State cand{u.h + scale * a.k[o], u.hu + scale * a.k[o + plane],
+                         u.hv + scale * a.k[o + 2 * plane]};
         if (a.mode == 2) {  // predictor forward, solver.py:639
             const State p = clean_and_limit(u, cand, a.kc, a.positivity != 0);
             a.P[o] = p.h;
@@ -469,7 +473,7 @@ __global__ void adj_pointwise_kernel(const PwArgs a) {
             const size_t on = (size_t)(a.nB == 1 ? 0 : b) * plane + i;
             State lqi;
             float ln = 0.0f;
-            friction_bwd(q, a.n[on], a.dt, a.friction_model, a.kc, lq, lqi, ln);
+            friction_bwd(q, a.n[on], dt, a.friction_model, a.kc, lq, lqi, ln);
             lq = lqi;
             if (a.nB == 1 && a.B > 1) atomicAdd(&a.ln[on], ln);
             else a.ln[on] += ln;
@@ -480,9 +484,9 @@ __global__ void adj_pointwise_kernel(const PwArgs a) {
         a.lU[o] += lold.h + lcand.h;
         a.lU[o + plane] += lold.hu + lcand.hu;
         a.lU[o + 2 * plane] += lold.hv + lcand.hv;
-        a.lk[o] = lcand.h * a.scale;
-        a.lk[o + plane] = lcand.hu * a.scale;
-        a.lk[o + 2 * plane] = lcand.hv * a.scale;
+        a.lk[o] = lcand.h * scale;
+        a.lk[o + plane] = lcand.hu * scale;
+        a.lk[o + 2 * plane] = lcand.hv * scale;
     }
 }
 
@@ -534,10 +538,10 @@ extern "C" int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, i
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
-extern "C" int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float* n,
-                                     int nB, int B, int ny, int nx, const swe_params* p, float dt,
-                                     const float* lam_out, float* lam_U, float* lam_k,
-                                     float* lam_n, float* P_out, void* stream) {
+namespace {
+int adj_pointwise(int mode, const float* U, const float* k, const float* n, int nB, int B, int ny,
+                  int nx, const swe_params* p, float dt, const float* dt_dev, const float* lam_out,
+                  float* lam_U, float* lam_k, float* lam_n, float* P_out, void* stream) {
     if (mode < 0 || mode > 2 || !U || !k || !valid_params(p) || B < 1 || ny < 1 || nx < 1)
         return SWE_EARG;
     if (mode == 2 && !P_out) return SWE_EARG;
@@ -554,6 +558,7 @@ extern "C" int swe_adj_pointwise_f32(int mode, const float* U, const float* k, c
     a.P = P_out;
     a.dt = dt;
     a.scale = mode == 0 ? dt : 0.5f * dt;
+    a.dt_dev = dt_dev;
     a.B = B;
     a.nB = nB;
     a.ny = ny;
@@ -565,4 +570,22 @@ extern "C" int swe_adj_pointwise_f32(int mode, const float* U, const float* k, c
     a.kc = make_consts(*p);
     adj_pointwise_kernel<<<blocks_for((long long)B * ny * nx), ADJ_THREADS, 0, (cudaStream_t)stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+}  // namespace
+
+extern "C" int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float* n,
+                                     int nB, int B, int ny, int nx, const swe_params* p, float dt,
+                                     const float* lam_out, float* lam_U, float* lam_k,
+                                     float* lam_n, float* P_out, void* stream) {
+    return adj_pointwise(mode, U, k, n, nB, B, ny, nx, p, dt, nullptr, lam_out, lam_U, lam_k, lam_n,
+                         P_out, stream);
+}
+
+extern "C" int swe_adj_pointwise_dev_f32(int mode, const float* U, const float* k, const float* n,
+                                         int nB, int B, int ny, int nx, const swe_params* p,
+                                         const float* dt_dev, const float* lam_out, float* lam_U,
+                                         float* lam_k, float* lam_n, float* P_out, void* stream) {
+    if (!dt_dev) return SWE_EARG;
+    return adj_pointwise(mode, U, k, n, nB, B, ny, nx, p, 0.0f, dt_dev, lam_out, lam_U, lam_k, lam_n,
+                         P_out, stream);
 }

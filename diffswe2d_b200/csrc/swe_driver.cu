@@ -105,10 +105,230 @@ __global__ void clock_kernel(swe_clock* c, uint32_t* red, const float* series_t,
     }
 }
 
+// The gauge run's clock: each output interval is one forward() call of
+// duration out_dt with its own level (run mode), or a re-run of recorded
+// steps (replay mode).  Same double-precision bookkeeping as clock_kernel.
+__global__ void run_clock_kernel(swe_run_clock* rc, uint32_t* red, const float* levels, int levelB,
+                                 float* level_out, const float* U, const float* bed, int bedB,
+                                 int B, int ny, int nx, const int32_t* gauge_cells, int ngauge,
+                                 float* gauge_out, float* step_dt, int32_t* step_code) {
+    __shared__ int s_record;  // interval whose gauges are read from U, or -1
+    __shared__ int s_level;   // interval whose level the next step uses, or -1
+    const int tid = threadIdx.x;
+    swe_clock* c = &rc->base;
+    if (tid == 0) {
+        s_record = -1;
+        s_level = -1;
+        if (rc->replay) {
+            if (c->active) c->steps += 1;
+            const int s = c->steps;
+            if (s < rc->replay_end && s < rc->record_cap) {
+                c->max_dt = step_dt[s];
+                s_level = step_code[s] >> 1;
+                red[0] = 0u;
+                red[1] = 0u;
+                red[2] = 0u;
+                c->active = 1;
+            } else {
+                c->active = 0;
+            }
+        } else {
+            if (c->active) {
+                const uint32_t st = red[2];
+                const float dt = __uint_as_float(red[3]);
+                if (st & (SWE_S_NONFINITE_STATE | SWE_S_NONFINITE_DT | SWE_S_NONPOSITIVE_DT)) {
+                    c->state = SWE_CLOCK_FAILED;
+                    c->dt_status = st;
+                    c->last_dt = dt;
+                } else {
+                    double elapsed = c->elapsed + (double)dt;
+                    if (elapsed > c->duration && elapsed - c->duration <= c->tolerance)
+                        elapsed = c->duration;
+                    c->last_dt = dt;
+                    const int s = c->steps;
+                    const bool ends = c->duration - elapsed <= c->tolerance;
+                    if (s < rc->record_cap) {
+                        step_dt[s] = dt;
+                        step_code[s] = 2 * rc->chunk + (ends ? 1 : 0);
+                    }
+                    c->steps = s + 1;
+                    rc->chunk_steps += 1;
+                    c->elapsed = elapsed;
+                    if (ends) {
+                        s_record = rc->chunk;
+                        rc->chunk += 1;
+                        rc->chunk_steps = 0;
+                        c->elapsed = 0.0;
+                    }
+                }
+            }
+            if (c->state == SWE_CLOCK_RUNNING) {
+                if (rc->chunk >= rc->n_out) {
+                    c->state = SWE_CLOCK_DONE;
+                } else if (c->steps >= rc->record_cap) {
+                    c->state = SWE_CLOCK_RECORD_FULL;
+                } else if (rc->chunk_steps >= c->max_steps) {
+                    c->state = SWE_CLOCK_MAXSTEPS;
+                } else {
+                    // An interval that has not ended has remaining > tolerance.
+                    const double remaining = c->duration - c->elapsed;
+                    double step_max_dt = remaining;
+                    if (c->max_dt_cap > 0.0 && c->max_dt_cap < remaining) step_max_dt = c->max_dt_cap;
+                    c->max_dt = (float)step_max_dt;
+                    s_level = rc->chunk;
+                    red[0] = 0u;
+                    red[1] = 0u;
+                    red[2] = 0u;
+                }
+            }
+            c->active = c->state == SWE_CLOCK_RUNNING ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    const int rec = s_record, lev = s_level;
+    if (rec >= 0) {  // eta = h + bed at the gauges (after the interval's last step)
+        const size_t plane = (size_t)ny * nx;
+        for (int k = tid; k < B * ngauge; k += blockDim.x) {
+            const int b = k / ngauge, g = k - b * ngauge;
+            const size_t cell = (size_t)gauge_cells[2 * g] * nx + gauge_cells[2 * g + 1];
+            const float z = bed[(bedB == 1 ? 0 : (size_t)b) * plane + cell];
+            gauge_out[((size_t)b * rc->n_out + rec) * ngauge + g] = U[(size_t)b * 3 * plane + cell] + z;
+        }
+    }
+    if (lev >= 0)
+        for (int b = tid; b < levelB; b += blockDim.x) level_out[b] = levels[(size_t)lev * levelB + b];
+}
+
+// lam[b,0,cell_g] += g_gauge[b, c, g]; one thread per batch member, gauges in
+// order, so repeated gauge cells accumulate deterministically.
+__global__ void gauge_adjoint_kernel(float* lam, int B, int ny, int nx, const int32_t* gauge_cells,
+                                     int ngauge, const float* g_gauge, int n_out, int c) {
+    const size_t plane = (size_t)ny * nx;
+    for (int b = threadIdx.x; b < B; b += blockDim.x)
+        for (int g = 0; g < ngauge; ++g) {
+            const size_t cell = (size_t)gauge_cells[2 * g] * nx + gauge_cells[2 * g + 1];
+            lam[(size_t)b * 3 * plane + cell] += g_gauge[((size_t)b * n_out + c) * ngauge + g];
+        }
+}
+
+__global__ void gauge_adjoint_prep_kernel(const int32_t* cursor, const float* step_dt,
+                                          const int32_t* step_code, const float* levels, int levelB,
+                                          float* dt_out, float* level_out, float* lam, int B, int ny,
+                                          int nx, const int32_t* gauge_cells, int ngauge,
+                                          const float* g_gauge, int n_out, int nsteps) {
+    const int s = *cursor;
+    if (s < 0 || s >= nsteps) return;  // outside the record: nothing to set up
+    const int code = step_code[s];
+    const int c = code >> 1;
+    if (threadIdx.x == 0) dt_out[0] = step_dt[s];
+    for (int b = threadIdx.x; b < levelB; b += blockDim.x) level_out[b] = levels[(size_t)c * levelB + b];
+    if (code & 1) {
+        const size_t plane = (size_t)ny * nx;
+        for (int b = threadIdx.x; b < B; b += blockDim.x)
+            for (int g = 0; g < ngauge; ++g) {
+                const size_t cell = (size_t)gauge_cells[2 * g] * nx + gauge_cells[2 * g + 1];
+                lam[(size_t)b * 3 * plane + cell] += g_gauge[((size_t)b * n_out + c) * ngauge + g];
+            }
+    }
+}
+
+// One warp per batch member sums its partial sums in a fixed order.
+__global__ void gauge_adjoint_post_kernel(int32_t* cursor, const int32_t* step_code,
+                                          const float* parts, int nparts, int B, int blocks,
+                                          int levelB, float* g_levels, int nsteps) {
+    __shared__ float s_sum[32];
+    __shared__ int s_step;
+    if (threadIdx.x == 0) s_step = *cursor;
+    __syncthreads();  // every thread has the step before thread 0 moves the cursor
+    const int s = s_step;
+    if (s < 0 || s >= nsteps) return;
+    const int c = step_code[s] >> 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float total = 0.0f;  // levelB == 1: sum over members (thread 0)
+    for (int b0 = 0; b0 < B; b0 += nw) {
+        const int b = b0 + warp;
+        float v = 0.0f;
+        if (b < B)
+            for (int q = 0; q < nparts; ++q)
+                for (int k = lane; k < blocks; k += 32) v += parts[((size_t)q * B + b) * blocks + k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (levelB > 1) {
+            if (b < B && lane == 0) g_levels[(size_t)c * levelB + b] += v;
+        } else {
+            if (lane == 0) s_sum[warp] = b < B ? v : 0.0f;
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int w = 0; w < nw; ++w) total += s_sum[w];
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (levelB == 1) g_levels[c] += total;
+        *cursor = s - 1;
+    }
+}
+
 }  // namespace
 }  // namespace swe
 
 using namespace swe;
+
+extern "C" int swe_gauge_adjoint_prep_f32(const int32_t* cursor, const float* step_dt,
+                                          const int32_t* step_code, const float* levels, int levelB,
+                                          float* dt_out, float* level_out, float* lam, int B, int ny,
+                                          int nx, const int32_t* gauge_cells, int ngauge,
+                                          const float* g_gauge, int n_out, int nsteps,
+                                          void* stream) {
+    if (!cursor || !step_dt || !step_code || !levels || levelB < 1 || !dt_out || !level_out || !lam ||
+        B < 1 || ny < 1 || nx < 1 || ngauge < 0 || n_out < 1 || nsteps < 0)
+        return SWE_EARG;
+    if (ngauge > 0 && (!gauge_cells || !g_gauge)) return SWE_EARG;
+    gauge_adjoint_prep_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(
+        cursor, step_dt, step_code, levels, levelB, dt_out, level_out, lam, B, ny, nx, gauge_cells,
+        ngauge, g_gauge, n_out, nsteps);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_gauge_adjoint_post_f32(int32_t* cursor, const int32_t* step_code,
+                                          const float* parts, int nparts, int B, int blocks,
+                                          int levelB, float* g_levels, int nsteps, void* stream) {
+    if (!cursor || !step_code || !parts || nparts < 1 || B < 1 || blocks < 1 || !g_levels ||
+        (levelB != 1 && levelB != B) || nsteps < 0)
+        return SWE_EARG;
+    gauge_adjoint_post_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(cursor, step_code, parts, nparts,
+                                                                   B, blocks, levelB, g_levels,
+                                                                   nsteps);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_run_clock_f32(swe_run_clock* clock, uint32_t* red, const float* levels,
+                                 int levelB, float* level_out, const float* U, const float* bed,
+                                 int bedB, int B, int ny, int nx, const int32_t* gauge_cells,
+                                 int ngauge, float* gauge_out, float* step_dt, int32_t* step_code,
+                                 void* stream) {
+    if (!clock || !red || !levels || !level_out || levelB < 1 || !step_dt || !step_code)
+        return SWE_EARG;
+    if (B < 1 || ny < 1 || nx < 1 || ngauge < 0 || !U) return SWE_EARG;
+    if (levelB != 1 && levelB != B) return SWE_EARG;
+    if (ngauge > 0 && (!gauge_cells || !gauge_out || !bed || (bedB != 1 && bedB != B)))
+        return SWE_EARG;
+    run_clock_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(clock, red, levels, levelB, level_out, U,
+                                                          bed, bedB, B, ny, nx, gauge_cells, ngauge,
+                                                          gauge_out, step_dt, step_code);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+
+extern "C" int swe_gauge_adjoint_f32(float* lam, int B, int ny, int nx, const int32_t* gauge_cells,
+                                     int ngauge, const float* g_gauge, int n_out, int c,
+                                     void* stream) {
+    if (!lam || B < 1 || ny < 1 || nx < 1 || ngauge < 0 || n_out < 1 || c < 0 || c >= n_out)
+        return SWE_EARG;
+    if (ngauge == 0) return SWE_OK;
+    if (!gauge_cells || !g_gauge) return SWE_EARG;
+    gauge_adjoint_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(lam, B, ny, nx, gauge_cells, ngauge,
+                                                              g_gauge, n_out, c);
+    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
 
 extern "C" int swe_clock_f32(swe_clock* clock, uint32_t* red, const float* series_t,
                              const float* series_w, int nseries, float* level_out, const float* U,

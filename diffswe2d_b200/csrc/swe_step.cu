@@ -588,6 +588,14 @@ struct EnsCtl {
     const float* series_w;
     float* Ua;                 // state buffers: step n reads U[n & 1]
     float* Ub;
+    // interval mode (n_out > 0)
+    double out_dt, elapsed, tol, cap;
+    int n_out, chunk, ngauge, nx;
+    float max_dt_cur;          // max_dt of the current step (both modes)
+    const float* out_levels;
+    const int32_t* gauge_cells;
+    float* gauge_out;
+    const float* bed;
 };
 
 struct EnsGlobal {
@@ -652,15 +660,44 @@ __device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
         }
         c->time += (double)dt;
         c->dt_last = dt;
-        c->step += 1;
-        if (c->step >= c->steps) {
-            c->finished = 1;
+        const int done_step = c->step;
+        c->step = done_step + 1;
+        int fin = 0;
+        if (c->n_out > 0) {
+            // the interval bookkeeping of swe_run_clock_f32 (solver.py:741-768)
+            double el = c->elapsed + (double)dt;
+            if (el > c->out_dt && el - c->out_dt <= c->tol) el = c->out_dt;
+            if (c->out_dt - el <= c->tol) {
+                const float* Unew = (done_step & 1) ? c->Ua : c->Ub;  // this step's output
+                for (int q = 0; q < c->ngauge; ++q) {
+                    const size_t cell = (size_t)c->gauge_cells[2 * q] * c->nx + c->gauge_cells[2 * q + 1];
+                    c->gauge_out[(size_t)c->chunk * c->ngauge + q] = __ldcg(Unew + cell) + c->bed[cell];
+                }
+                c->chunk += 1;
+                el = 0.0;
+                if (c->chunk >= c->n_out) fin = 1;
+            }
+            c->elapsed = el;
+            if (!fin && c->step >= c->steps) {
+                c->status = SWE_S_STEP_LIMIT;
+                fin = 2;
+            }
+            if (!fin) {
+                const double rem = c->out_dt - el;
+                c->max_dt_cur = (float)((c->cap > 0.0 && c->cap < rem) ? c->cap : rem);
+                c->level = c->out_levels[c->chunk];
+            }
+        } else {
+            if (c->step >= c->steps) fin = 1;
+            else c->level = ens_level(*c);
+        }
+        if (fin) {
+            c->finished = fin;
             __threadfence();
             atomicAdd(&g->finished, 1u);
             atomicAdd(&g->progress, 1u);
             return;
         }
-        c->level = ens_level(*c);
         for (int w = 0; w < SWE_RED_WORDS; ++w) c->red[w] = 0u;
     }
     __threadfence();
@@ -735,6 +772,7 @@ ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGl
         if (threadIdx.x == 0) {
             sa.U = (step & 1) ? c->Ub : c->Ua;
             sa.U_out = (step & 1) ? c->Ua : c->Ub;
+            sa.max_dt = __ldcg(&c->max_dt_cur);
         }
         __syncthreads();
         const int nbx = c->nbx, rows = c->rows;
@@ -770,7 +808,14 @@ __global__ void ensemble_init_kernel(EnsCtl* ctl, int count, EnsGlobal* g) {
         c->status = 0u;
         c->time = 0.0;
         c->dt_last = 0.0f;
-        c->level = ens_level(*c);
+        if (c->n_out > 0) {
+            c->chunk = 0;
+            c->elapsed = 0.0;
+            c->max_dt_cur = (float)((c->cap > 0.0 && c->cap < c->out_dt) ? c->cap : c->out_dt);
+            c->level = c->out_levels[0];
+        } else {
+            c->level = ens_level(*c);
+        }
         if (c->finished) atomicAdd(&g->finished, 1u);
     }
 }
@@ -1041,8 +1086,11 @@ extern "C" int swe_ensemble_prepare_f32(const swe_ensemble_member* members, int 
         const swe_ensemble_member& e = members[m];
         StepArgs a{};
         const int fric = e.params.apply_friction ? 1 + e.params.friction_model : 0;
+        const bool interval = e.n_out > 0;
         if (fric != fric0 || !e.U_a || !e.U_b || !e.k1 || e.steps < 0 || e.rows < 1 ||
-            (e.nseries > 0 && (!e.series_t || !e.series_w)) ||
+            (!interval && e.nseries > 0 && (!e.series_t || !e.series_w)) || e.n_out < 0 ||
+            (interval && (!(e.out_dt > 0.0) || !e.out_levels || e.ngauge < 0 ||
+                          (e.ngauge > 0 && (!e.gauge_cells || !e.gauge_out)))) ||
             !fill_common(a, e.U_a, e.bed, 1, 1, e.ny, e.nx, &e.params, e.U_a, 1) ||
             (e.params.apply_friction && !e.n)) {
             rc = SWE_EARG;
@@ -1073,6 +1121,32 @@ extern "C" int swe_ensemble_prepare_f32(const swe_ensemble_member* members, int 
         c.start = e.start_time;
         c.Ua = e.U_a;
         c.Ub = e.U_b;
+        c.max_dt_cur = (float)e.max_dt;
+        if (interval) {
+            // gauge cells must lie in the grid (read back once per member)
+            int32_t cells[2 * SWE_ENSEMBLE_MAX_GAUGES];
+            if (e.ngauge > SWE_ENSEMBLE_MAX_GAUGES) {
+                rc = SWE_EARG;
+            } else if (e.ngauge > 0) {
+                if (cudaMemcpy(cells, e.gauge_cells, sizeof(int32_t) * 2 * e.ngauge,
+                               cudaMemcpyDeviceToHost) != cudaSuccess)
+                    rc = SWE_ECUDA;
+                for (int q = 0; q < e.ngauge && rc == SWE_OK; ++q)
+                    if (cells[2 * q] < 0 || cells[2 * q] >= e.ny || cells[2 * q + 1] < 0 ||
+                        cells[2 * q + 1] >= e.nx)
+                        rc = SWE_EARG;
+            }
+            c.n_out = e.n_out;
+            c.out_dt = e.out_dt;
+            c.tol = e.out_dt * 1e-12 > 1e-12 ? e.out_dt * 1e-12 : 1e-12;
+            c.cap = e.max_dt;
+            c.ngauge = e.ngauge;
+            c.nx = e.nx;
+            c.out_levels = e.out_levels;
+            c.gauge_cells = e.gauge_cells;
+            c.gauge_out = e.gauge_out;
+            c.bed = e.bed;
+        }
         ctl[m] = c;
     }
     if (rc == SWE_OK) {
@@ -1141,6 +1215,8 @@ extern "C" int swe_tune_sweep_rows(int rows) {
     g_sweep_rows = rows;
     return SWE_OK;
 }
+
+extern "C" int swe_sweep_rows(void) { return g_sweep_rows; }
 
 extern "C" int swe_load_kernels(void) {
     // Touching each kernel loads its module now (CUDA lazy loading), so that

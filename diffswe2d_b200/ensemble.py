@@ -158,3 +158,127 @@ class Ensemble:
             h is not None for h in self.hmax) else None
         total = sum(c * s for c, s in zip(self.cells, steps))
         return EnsembleResult(states, steps, times, hmax, e0.elapsed_time(e1), total)
+
+
+@dataclass
+class GaugeEnsembleResult:
+    gauges: torch.Tensor   # [M, n_out, ngauge] eta after each output interval
+    states: torch.Tensor   # [M, 3, ny, nx] final states
+    steps: List[int]
+    times: List[float]
+    elapsed_ms: float      # device time of the persistent launch
+    cell_updates: int
+
+    @property
+    def mcells_per_s(self) -> float:
+        return self.cell_updates / (self.elapsed_ms * 1e-3) / 1e6
+
+
+class GaugeEnsemble:
+    """Members of one grid shape in interval mode: member m runs ``n_out``
+    output intervals of ``out_dt`` seconds with levels ``out_levels[m]``, each
+    interval exactly like ``SWE2D.forward(U, t_end=out_dt,
+    boundary_level=level)`` with its own CFL steps, and records eta = h + bed
+    at the gauge cells after every interval -- the run of
+    ``gauge_run`` for a batch of one, for up to 1024 members in one persistent
+    launch (the solver-generated training runs of the learned warm start).
+
+    bed [M, ny, nx]; n [M or 1, ny, nx]; U0 [M, 3, ny, nx]; out_levels
+    [M, n_out] (float32, device tensors).
+    """
+
+    def __init__(self, bed: torch.Tensor, n: torch.Tensor, U0: torch.Tensor, out_levels: torch.Tensor,
+                 out_dt: float, gauges: Sequence, config: SWEConfig, dx: float, dy: Optional[float] = None,
+                 rows: Optional[int] = None, max_steps: int = 1 << 30, max_dt_cap: float = 0.0):
+        from .autotune import tuned_rows
+        M, ny, nx = bed.shape
+        if not 1 <= M <= 1024:
+            raise ValueError("a gauge ensemble holds 1 to 1024 members")
+        if U0.shape != (M, 3, ny, nx) or out_levels.ndim != 2 or out_levels.shape[0] != M:
+            raise ValueError("U0 must be [M,3,ny,nx] and out_levels [M,n_out] for bed [M,ny,nx]")
+        if n.ndim != 3 or n.shape[0] not in (1, M) or n.shape[1:] != (ny, nx):
+            raise ValueError("n must be [1 or M, ny, nx]")
+        if not out_dt > 0:
+            raise ValueError("out_dt must be positive")
+        if not 0 <= len(gauges) <= 64:
+            raise ValueError("at most 64 gauges")
+        for iy, ix in gauges:
+            if not (0 <= iy < ny and 0 <= ix < nx):
+                raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
+        dev = bed.device
+        self.device = dev
+        self.M, self.ny, self.nx = M, ny, nx
+        self.n_out = out_levels.shape[1]
+        self.ngauge = len(gauges)
+        self.bed = nat.require_cuda_f32("bed", bed)
+        self.n = nat.require_cuda_f32("n", n)
+        self.levels = nat.require_cuda_f32("out_levels", out_levels)
+        self.initial = nat.require_cuda_f32("U0", U0)
+        self.Ua = self.initial.clone()
+        self.Ub = torch.empty_like(self.Ua)
+        self.k1 = torch.empty_like(self.Ua)
+        self.cells = torch.tensor([v for g in gauges for v in g] or [0, 0], dtype=torch.int32,
+                                  device=dev)
+        self.gauge_out = torch.zeros((M, self.n_out, max(self.ngauge, 1)), device=dev)
+        self.friction = (1 + (0 if config.frictionmodel == "manning" else 1)) if config.apply_friction else 0
+        r = int(rows) if rows is not None else tuned_rows(ny * nx, dev)
+        p = nat.params(config, dx, dx if dy is None else dy)
+        members = (nat.SweEnsembleMember * M)()
+        for m in range(M):
+            mem = members[m]
+            mem.bed = self.bed[m].data_ptr()
+            mem.n = self.n[m if self.n.shape[0] == M else 0].data_ptr()
+            mem.U_a, mem.U_b, mem.k1 = self.Ua[m].data_ptr(), self.Ub[m].data_ptr(), self.k1[m].data_ptr()
+            mem.hmax = None
+            mem.nseries, mem.ny, mem.nx, mem.steps, mem.rows = 0, ny, nx, int(max_steps), r
+            mem.level = 0.0
+            mem.start_time = 0.0
+            mem.max_dt = float(max_dt_cap)
+            mem.params = p
+            mem.out_dt = float(out_dt)
+            mem.n_out = self.n_out
+            mem.ngauge = self.ngauge
+            mem.out_levels = self.levels[m].data_ptr()
+            mem.gauge_cells = self.cells.data_ptr()
+            mem.gauge_out = self.gauge_out[m].data_ptr()
+        lib = nat.lib()
+        self.workspace = torch.empty(int(lib.swe_ensemble_workspace_bytes(M)), dtype=torch.uint8,
+                                     device=dev)
+        self.results_dev = torch.empty(M * ctypes.sizeof(nat.SweEnsembleResult), dtype=torch.uint8,
+                                       device=dev)
+        self.error_dev = torch.zeros(1, dtype=torch.int32, device=dev)
+        nat.check(lib.swe_ensemble_prepare_f32(members, M, nat.ptr(self.workspace),
+                                               nat.stream_handle(dev)), "gauge ensemble prepare")
+        self.blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 6
+
+    def run(self) -> GaugeEnsembleResult:
+        lib, st = nat.lib(), nat.stream_handle(self.device)
+        self.Ua.copy_(self.initial)
+        self.gauge_out.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nat.check(lib.swe_ensemble_reset_f32(nat.ptr(self.workspace), self.M, st), "ensemble reset")
+        e0.record()
+        nat.check(lib.swe_ensemble_run_f32(nat.ptr(self.workspace), self.M, self.friction, self.blocks,
+                                           st), "ensemble run")
+        e1.record()
+        nat.check(lib.swe_ensemble_results_f32(nat.ptr(self.workspace), self.M,
+                                               nat.ptr(self.results_dev), nat.ptr(self.error_dev), st),
+                  "ensemble results")
+        torch.cuda.synchronize(self.device)
+        res = (nat.SweEnsembleResult * self.M).from_buffer_copy(bytes(self.results_dev.cpu().numpy()))
+        if int(self.error_dev.item()) != 0:
+            raise RuntimeError("ensemble kernel stopped: idle limit reached")
+        steps, times = [], []
+        final = torch.empty_like(self.Ua)
+        for m in range(self.M):
+            r = res[m]
+            if r.finished == 2:
+                if r.status & nat.S_STEP_LIMIT:
+                    raise RuntimeError(f"member {m}: step cap reached before the last output interval")
+                raise FloatingPointError(f"member {m}: time step failed (status {r.status})")
+            final[m] = self.Ua[m] if r.steps % 2 == 0 else self.Ub[m]
+            steps.append(int(r.steps))
+            times.append(float(r.time))
+        cells = self.ny * self.nx
+        return GaugeEnsembleResult(self.gauge_out[..., : self.ngauge].clone(), final, steps, times,
+                                   e0.elapsed_time(e1), cells * sum(steps))

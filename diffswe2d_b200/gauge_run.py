@@ -1,0 +1,342 @@
+"""A whole gauge run -- the model advanced through ``n_out`` output intervals,
+each with its own boundary level, gauges read after each interval -- as one
+autograd node.
+
+The reference's inversion script runs this loop in Python
+(``Examples/inverse/Monai_Valley/Monai_Velley_BC_inversion_spline_lr002/
+bc_inversion_train.py:332-411``): one ``SWE2D.forward(U, t_end=dt_out,
+boundary_level=series[i])`` call per output interval, gauges read from the
+state after each call, autograd through everything (optionally
+``torch.utils.checkpoint`` per chunk).  Here:
+
+* forward: the device-driven time loop (``swe_run_clock_f32`` between
+  clocked steps) captured in a CUDA graph of ``graph_steps`` steps and
+  replayed until the clock reports the end; every interval's level is read
+  on the device, every step's dt and interval are recorded on the device,
+  and the state is copied to a checkpoint every ``checkpoint_every`` steps.
+  No host synchronisation inside the run except one clock read per replay.
+* backward: segment by segment in reverse, the segment's states are
+  recomputed from its checkpoint in replay mode (bit for bit the forward's
+  states), then the hand-written step adjoint runs in reverse over the
+  segment with the gauge cotangents injected at the end of each interval.
+
+Gradients flow to the initial state, the per-interval levels and the
+roughness field, as through the reference's loop (dt detached).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence, Tuple
+
+import torch
+
+from . import _native as nat
+from .adjoint import LEVEL_BLOCKS, AdjointStepper, _check_no_bed_grad
+
+GRAPH_STEPS = 32
+CHECKPOINT_EVERY = 128
+
+
+class GaugeRunWorkspace:
+    """Device buffers and captured graphs of gauge runs of one model, state
+    shape, interval count and gauge set."""
+
+    def __init__(self, model, B: int, ny: int, nx: int, dev, levelB: int, n_out: int,
+                 gauges: Sequence[Tuple[int, int]], graph_steps: int = GRAPH_STEPS,
+                 checkpoint_every: int = CHECKPOINT_EVERY, record_cap: Optional[int] = None):
+        if graph_steps < 2 or graph_steps % 2:
+            raise ValueError("graph_steps must be even and >= 2")
+        if checkpoint_every < graph_steps or checkpoint_every % graph_steps:
+            raise ValueError("checkpoint_every must be a multiple of graph_steps")
+        self.model = model
+        self.B, self.ny, self.nx, self.dev = B, ny, nx, dev
+        self.levelB, self.n_out = levelB, n_out
+        self.G, self.k = graph_steps, checkpoint_every
+        shape = (B, 3, ny, nx)
+        self.bufs = [torch.empty(shape, device=dev), torch.empty(shape, device=dev)]
+        self.scratch = torch.empty(shape, device=dev)
+        self.red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+        probe = torch.empty(shape, device=dev)
+        bed, n = model._fields(probe)
+        self.bed = torch.empty_like(bed)
+        self.n = torch.empty_like(n)
+        self.levels = torch.zeros((n_out, levelB), device=dev)
+        self.lv = torch.zeros(levelB, device=dev)
+        self.ngauge = len(gauges)
+        for iy, ix in gauges:
+            if not (0 <= iy < ny and 0 <= ix < nx):
+                raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
+        self.cells = torch.tensor([v for g in gauges for v in g] or [0, 0], dtype=torch.int32,
+                                  device=dev)
+        self.gauge_out = torch.zeros((B, n_out, max(self.ngauge, 1)), device=dev)
+        self.record_cap = int(record_cap) if record_cap else max(4096, 64 * n_out)
+        self.step_dt = torch.zeros(self.record_cap, device=dev)
+        self.step_code = torch.zeros(self.record_cap, dtype=torch.int32, device=dev)
+        self.clock = torch.zeros(ctypes.sizeof(nat.SweRunClock), dtype=torch.uint8, device=dev)
+        self.params = model._params()
+        self.ckpts = []
+        self.seg = None
+        self.fwd_graph = None
+        self.replay_graph = None
+        self.last_steps = 0
+        self.generation = 0
+        self.stepper = None
+        from .autotune import tuned_rows_for_shape
+        self.rows = tuned_rows_for_shape(B, ny, nx, dev)
+
+    # ------------------------------------------------------------ launches
+    def _tick(self, state):
+        rc = nat.lib().swe_run_clock_f32(
+            nat.ptr(self.clock), nat.ptr(self.red), nat.ptr(self.levels), self.levelB,
+            nat.ptr(self.lv), nat.ptr(state), nat.ptr(self.bed), self.bed.shape[0], self.B, self.ny,
+            self.nx, nat.ptr(self.cells), self.ngauge, nat.ptr(self.gauge_out), nat.ptr(self.step_dt),
+            nat.ptr(self.step_code), nat.stream_handle(self.dev))
+        nat.check(rc, "gauge-run clock")
+
+    def _step(self, src, dst):
+        rc = nat.lib().swe_step_clocked_f32(
+            3, nat.ptr(src), nat.ptr(self.bed), self.bed.shape[0], nat.ptr(self.n), self.n.shape[0],
+            self.B, self.ny, self.nx, self.params, nat.ptr(self.lv), self.levelB, nat.ptr(self.clock),
+            None, nat.FORCING_NONE, 1, nat.ptr(self.scratch), nat.ptr(self.red), nat.ptr(dst), None,
+            nat.stream_handle(self.dev))
+        nat.check(rc, "gauge-run step")
+        self._tick(dst)
+
+    def _set_clock(self, **fields):
+        c = nat.SweRunClock()
+        c.base.duration = self.out_dt
+        c.base.tolerance = max(1e-12, 1e-12 * abs(self.out_dt))
+        c.base.max_dt_cap = self.max_dt_cap
+        c.base.max_steps = self.max_steps
+        c.out_dt = self.out_dt
+        c.n_out = self.n_out
+        c.record_cap = self.record_cap
+        for k, v in fields.items():
+            if k in ("steps", "active"):
+                setattr(c.base, k, v)
+            else:
+                setattr(c, k, v)
+        self.clock.copy_(torch.frombuffer(bytearray(bytes(c)), dtype=torch.uint8))
+
+    def _read_clock(self) -> nat.SweRunClock:
+        return nat.SweRunClock.from_buffer_copy(self.clock.cpu().numpy().tobytes())
+
+    # ------------------------------------------------------------- forward
+    def run(self, U0, levels, out_dt: float, max_dt_cap=None, max_steps: int = 1_000_000):
+        """Forward gauge run; returns (gauges [B, n_out, ngauge], final state).
+        Both are views of workspace buffers (valid until the next run)."""
+        bed, n = self.model._fields(U0)
+        self.bed.copy_(bed)
+        self.n.copy_(n)
+        self.levels.copy_(levels)
+        self.out_dt = float(out_dt)
+        self.max_dt_cap = float(max_dt_cap) if max_dt_cap is not None else 0.0
+        self.max_steps = int(max_steps)
+        self.generation += 1
+        self.bufs[0].copy_(U0)
+        self.gauge_out.zero_()
+        self._set_clock()
+        self._tick(self.bufs[0])
+        if self.fwd_graph is None:
+            from .autotune import sweep_rows
+            nat.load_kernels()
+            g = torch.cuda.CUDAGraph()
+            with sweep_rows(self.rows), torch.cuda.graph(g):
+                for s in range(self.G):
+                    self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
+            self.fwd_graph = g
+        per_ckpt = self.k // self.G
+        replay = 0
+        while True:
+            if replay % per_ckpt == 0:
+                j = replay // per_ckpt
+                if j == len(self.ckpts):
+                    self.ckpts.append(torch.empty_like(self.bufs[0]))
+                self.ckpts[j].copy_(self.bufs[0])
+            self.fwd_graph.replay()
+            replay += 1
+            c = self._read_clock()
+            if c.base.state != nat.CLOCK_RUNNING:
+                break
+        if c.base.state == nat.CLOCK_FAILED:
+            self.model._raise_on_status(int(c.base.dt_status), float(c.base.last_dt))
+        if c.base.state == nat.CLOCK_MAXSTEPS:
+            raise RuntimeError(f"Reached max_steps={self.max_steps} before an output interval of "
+                               f"{self.out_dt} s was complete.")
+        if c.base.state == nat.CLOCK_RECORD_FULL:
+            raise _RecordFull(int(c.base.steps))
+        self.last_steps = int(c.base.steps)
+        return self.gauge_out[..., : self.ngauge], self.bufs[0]
+
+    # ------------------------------------------------------------ backward
+    def _recompute_segment(self, j: int, s0: int, s1: int):
+        """States entering steps s0 .. s1-1 into self.seg[0 .. s1-s0-1]."""
+        if self.seg is None:
+            self.seg = [torch.empty_like(self.bufs[0]) for _ in range(self.k + 1)]
+        self.seg[0].copy_(self.ckpts[j])
+        self._set_clock(replay=1, replay_end=s1, steps=s0, active=0)
+        self._tick(self.seg[0])
+        if self.replay_graph is None:
+            from .autotune import sweep_rows
+            g = torch.cuda.CUDAGraph()
+            with sweep_rows(self.rows), torch.cuda.graph(g):
+                for i in range(self.k):
+                    self._step(self.seg[i], self.seg[i + 1])
+            self.replay_graph = g
+        self.replay_graph.replay()
+
+    def _alloc_backward(self):
+        dev, shape = self.dev, self.bufs[0].shape
+        self.stepper = AdjointStepper(self.model, self.B, self.ny, self.nx, dev, self.levelB)
+        self.lam = [torch.empty(shape, device=dev), torch.empty(shape, device=dev)]
+        self.g_gauge = torch.zeros_like(self.gauge_out)
+        self.g_levels = torch.zeros_like(self.levels)
+        self.lam_n = torch.zeros_like(self.n) if self.stepper.fric else None
+        self.cursor = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.dt_cur = torch.zeros(1, device=dev)
+        self.lv_cur = torch.zeros(self.levelB, device=dev)
+        self.adj_graph = None
+
+    def _adjoint_steps(self, count):
+        """Enqueue the adjoint of the steps in seg slots count-1 .. 0, the
+        step index taken from the device cursor (decremented per step); lam
+        alternates lam[0] -> lam[1] -> ..., starting from lam[0]."""
+        lib, st, stp = nat.lib(), nat.stream_handle(self.dev), self.stepper
+        for q, i in enumerate(range(count - 1, -1, -1)):
+            lam_in, lam_out = self.lam[q % 2], self.lam[1 - q % 2]
+            rc = lib.swe_gauge_adjoint_prep_f32(
+                nat.ptr(self.cursor), nat.ptr(self.step_dt), nat.ptr(self.step_code),
+                nat.ptr(self.levels), self.levelB, nat.ptr(self.dt_cur), nat.ptr(self.lv_cur),
+                nat.ptr(lam_in), self.B, self.ny, self.nx, nat.ptr(self.cells), self.ngauge,
+                nat.ptr(self.g_gauge), self.n_out, self.record_cap, st)
+            nat.check(rc, "gauge-run adjoint setup")
+            lam_out.zero_()
+            part = stp(self.seg[i], self.lv_cur, self.dt_cur, lam_in, lam_out, self.lam_n)
+            rc = lib.swe_gauge_adjoint_post_f32(
+                nat.ptr(self.cursor), nat.ptr(self.step_code), nat.ptr(part), 2, self.B,
+                LEVEL_BLOCKS, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)
+            nat.check(rc, "gauge-run adjoint finish")
+
+    def backward(self, g_gauges, g_final):
+        """Adjoints of U0, the levels [n_out, levelB] and the roughness field
+        for the cotangents of the gauges [B, n_out, ngauge] and of the final
+        state (either may be None).  The last segment's adjoint steps are
+        enqueued directly; every full segment replays one captured graph of
+        checkpoint_every adjoint steps.  No host synchronisation."""
+        total = self.last_steps
+        if self.stepper is None:
+            self._alloc_backward()
+        if g_final is None:
+            self.lam[0].zero_()
+        else:
+            self.lam[0].copy_(g_final)
+        if g_gauges is None:
+            self.g_gauge.zero_()
+        else:
+            self.g_gauge[..., : self.ngauge].copy_(g_gauges)
+        self.g_levels.zero_()
+        if self.lam_n is not None:
+            self.lam_n.zero_()
+        nseg = (total + self.k - 1) // self.k
+        for j in range(nseg - 1, -1, -1):
+            s0, s1 = j * self.k, min((j + 1) * self.k, total)
+            self._recompute_segment(j, s0, s1)
+            self.cursor.fill_(s1 - 1)
+            count = s1 - s0
+            if count < self.k:
+                self._adjoint_steps(count)
+                if count % 2:
+                    self.lam[0].copy_(self.lam[1])
+                continue
+            if self.adj_graph is None:
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._adjoint_steps(self.k)
+                self.adj_graph = g
+                self.cursor.fill_(s1 - 1)  # the capture ran nothing; keep the cursor explicit
+            self.adj_graph.replay()
+        lam_n = self.lam_n.clone() if self.lam_n is not None else None
+        return self.lam[0].clone(), self.g_levels.clone(), lam_n
+
+
+class _RecordFull(RuntimeError):
+    def __init__(self, steps):
+        super().__init__(f"gauge run needs more than {steps} recorded steps")
+        self.steps = steps
+
+
+class _GaugeRunFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U0, levels, n, ws, out_dt, max_dt_cap, max_steps):
+        lv = levels.detach().t() if levels.ndim == 2 else levels.detach().reshape(-1, 1)
+        gauges, final = ws.run(U0.detach(), lv, out_dt, max_dt_cap, max_steps)
+        ctx.ws, ctx.generation = ws, ws.generation
+        ctx.levels_shape = levels.shape
+        return gauges.clone(), final.clone()
+
+    @staticmethod
+    def backward(ctx, g_gauges, g_final):
+        ws = ctx.ws
+        if ws.generation != ctx.generation:
+            raise RuntimeError("the gauge-run workspace ran again before this run's backward pass; "
+                               "call backward before the next gauge_run of the same shape")
+        lam, g_levels, lam_n = ws.backward(g_gauges, g_final)
+        g_lv = None
+        if ctx.needs_input_grad[1]:
+            g_lv = (g_levels.t() if len(ctx.levels_shape) == 2 else g_levels).reshape(ctx.levels_shape)
+        g_n = lam_n if (ctx.needs_input_grad[2] and lam_n is not None) else None
+        return lam if ctx.needs_input_grad[0] else None, g_lv, g_n, None, None, None, None
+
+
+_WORKSPACES = {}
+
+
+def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
+              gauges: Sequence[Tuple[int, int]], max_dt_cap=None, max_steps: int = 1_000_000,
+              graph_steps: int = GRAPH_STEPS, checkpoint_every: int = CHECKPOINT_EVERY):
+    """Advance ``U0`` through ``n_out`` output intervals of ``out_dt``
+    seconds; interval i runs exactly like ``model(U, t_end=out_dt,
+    boundary_level=level_i)``, with level_i = ``levels[:, i]`` for levels
+    [B, n_out] (one series per batch member) or ``levels[i]`` for [n_out].
+
+    Returns ``(gauges, U_final)``: eta = h + bed at the gauge cells (row,
+    column) after every interval, [B, n_out, len(gauges)], and the final
+    state.  Differentiable with respect to U0, levels and the roughness
+    field."""
+    _check_no_bed_grad(model)
+    model._check_state(U0)
+    U0 = nat.require_cuda_f32("U0", U0)
+    B, _, ny, nx = U0.shape
+    if levels.ndim == 2:
+        if levels.shape[0] != B:
+            raise ValueError(f"levels [B, n_out] must have B={B} rows, got {tuple(levels.shape)}")
+        levelB, n_out = B, levels.shape[1]
+    elif levels.ndim == 1:
+        levelB, n_out = 1, levels.shape[0]
+    else:
+        raise ValueError("levels must be [n_out] or [B, n_out]")
+    if n_out < 1:
+        raise ValueError("need at least one output interval")
+    if not out_dt > 0:
+        raise ValueError("out_dt must be positive")
+    key = (id(model), B, ny, nx, str(U0.device), levelB, n_out, tuple(map(tuple, gauges)),
+           graph_steps, checkpoint_every)
+    ws = _WORKSPACES.get(key)
+    if ws is None or ws.model is not model:
+        ws = GaugeRunWorkspace(model, B, ny, nx, U0.device, levelB, n_out, gauges, graph_steps,
+                               checkpoint_every)
+        _WORKSPACES.clear()
+        _WORKSPACES[key] = ws
+    levels_f = levels.to(dtype=torch.float32)
+    while True:
+        try:
+            return _GaugeRunFunction.apply(U0, levels_f, model.roughness_length, ws, float(out_dt),
+                                           max_dt_cap, int(max_steps))
+        except _RecordFull as e:
+            ws = GaugeRunWorkspace(model, B, ny, nx, U0.device, levelB, n_out, gauges, graph_steps,
+                                   checkpoint_every, record_cap=4 * e.steps)
+            _WORKSPACES.clear()
+            _WORKSPACES[key] = ws
+
+
+__all__ = ["gauge_run", "GaugeRunWorkspace", "GRAPH_STEPS", "CHECKPOINT_EVERY"]

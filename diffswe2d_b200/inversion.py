@@ -23,6 +23,7 @@ import numpy as np
 import torch
 
 from .adjoint import forward_checkpointed
+from .gauge_run import gauge_run
 
 
 # ------------------------------------------------------------------ spline
@@ -110,7 +111,16 @@ class InversionProblem:
 
     def simulate(self, series: torch.Tensor, differentiable: bool = True) -> torch.Tensor:
         """Gauge eta [B, n_out, n_gauges] after each output chunk; the chunk's
-        level is series[:, i] (held over the chunk, as the reference does)."""
+        level is series[:, i] (held over the chunk, as the reference does).
+        One gauge_run: a device-driven run with a checkpointed adjoint."""
+        if differentiable:
+            return gauge_run(self.model, self.U0, series, self.dt_out, self.gauges)[0]
+        with torch.no_grad():
+            return gauge_run(self.model, self.U0, series.detach(), self.dt_out, self.gauges)[0]
+
+    def simulate_chunked(self, series: torch.Tensor, differentiable: bool = True) -> torch.Tensor:
+        """The same run as the reference's script writes it: one forward()
+        call (one autograd node, forward_checkpointed) per output chunk."""
         U = self.U0
         out = []
         for i in range(self.n_out):
@@ -179,51 +189,112 @@ def invert(problem: InversionProblem, raw0: torch.Tensor, lr: float = 0.002, max
                            [None if r is None else r * per_it for r in reached], wall, losses)
 
 
+@dataclass
+class RunupFamily:
+    """The runup cases of one resolution: the runup bathymetry of the
+    scenario recipe (seeded) perturbed per case by three seeded Gaussian
+    bumps of amplitude up to ``bathy_perturb`` metres, walls except the west
+    water level, Manning n = 0.01, still water at rest; gauges at
+    ``n_gauges`` seeded cells deeper than 3 cm in the unperturbed bed (the
+    same cells for every case); a clamped cubic spline of ``n_controls``
+    controls sampled every ``dt_out`` seconds over ``duration``."""
+    ny: int = 122
+    nx: int = 196
+    dx: float = 0.028
+    seed: int = 0
+    duration: float = 22.5
+    dt_out: float = 0.02
+    n_controls: int = 16
+    n_gauges: int = 6
+    bathy_perturb: float = 0.01
+    device: str = "cuda"
+
+    def __post_init__(self):
+        from . import scenarios
+        from .config import SWEConfig
+        self.base = scenarios.runup(ny=self.ny, nx=self.nx, dx=self.dx, seed=self.seed)
+        self.config = SWEConfig(**self.base.config)
+        rng = np.random.default_rng(self.seed + 7919)
+        wet = np.argwhere(self.base.bed < -0.03)
+        pick = rng.choice(len(wet), size=self.n_gauges, replace=False)
+        self.gauges = [tuple(int(v) for v in wet[i]) for i in sorted(pick)]
+        self.n_out = int(round(self.duration / self.dt_out))
+        times = torch.arange(self.n_out, dtype=torch.float64) * self.dt_out
+        basis, _, _ = clamped_bspline_basis(times, self.n_controls, 3)
+        self.basis = basis.float().to(self.device)
+
+    def beds(self, count: int, rng) -> np.ndarray:
+        """[count, ny, nx] float32 perturbed beds."""
+        X, Y = np.meshgrid((np.arange(self.nx) + 0.5) * self.dx, (np.arange(self.ny) + 0.5) * self.dx)
+        out = np.empty((count, self.ny, self.nx), np.float32)
+        for c in range(count):
+            z = self.base.bed.astype(np.float64).copy()
+            if self.bathy_perturb > 0:
+                for _ in range(3):
+                    cx = rng.uniform(0.1, 0.9) * self.nx * self.dx
+                    cy = rng.uniform(0.1, 0.9) * self.ny * self.dx
+                    amp = rng.uniform(-self.bathy_perturb, self.bathy_perturb)
+                    sig = rng.uniform(0.05, 0.2)
+                    z += amp * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * sig ** 2))
+            out[c] = z
+        return out
+
+    def controls(self, count: int, rng) -> np.ndarray:
+        """[count, n_controls] control values uniform in [-0.012, 0.015] m."""
+        return rng.uniform(-0.012, 0.015, size=(count, self.n_controls)).astype(np.float32)
+
+    def problem(self, beds: np.ndarray, truth: Optional[np.ndarray] = None):
+        """InversionProblem over the cases of `beds` (batched); targets from
+        the forward run with control values `truth`, if given."""
+        from .solver import SWE2D
+        bed = torch.tensor(beds[:, None], device=self.device)
+        n = torch.full_like(bed, 0.01)
+        model = SWE2D(bed, n, self.dx, self.dx, config=self.config, train_dem=False)
+        h0 = torch.clamp(-bed, min=0.0)
+        U0 = torch.cat([h0, torch.zeros_like(h0), torch.zeros_like(h0)], dim=1).contiguous()
+        problem = InversionProblem(model, U0, self.gauges, self.dt_out, self.n_out, self.basis)
+        if truth is not None:
+            raw = raw_from_controls(torch.as_tensor(truth, device=self.device))
+            with torch.no_grad():
+                problem.targets = problem.simulate(problem.series(raw), differentiable=False)
+        return problem
+
+    def ensemble_gauges(self, beds: np.ndarray, values: np.ndarray, rows: Optional[int] = None):
+        """Gauge eta [count, n_out, n_gauges] of independent runs (each its own
+        CFL steps), in persistent-kernel launches of up to 1024 runs."""
+        from .ensemble import GaugeEnsemble
+        out = []
+        n = torch.full((1, self.ny, self.nx), 0.01, device=self.device)
+        for s in range(0, beds.shape[0], 1024):
+            bed = torch.tensor(beds[s:s + 1024], device=self.device)
+            h0 = torch.clamp(-bed, min=0.0)
+            U0 = torch.stack([h0, torch.zeros_like(h0), torch.zeros_like(h0)], dim=1).contiguous()
+            v = torch.as_tensor(values[s:s + 1024], device=self.device)
+            levels = (v @ self.basis.t()).contiguous()
+            ens = GaugeEnsemble(bed, n, U0, levels, self.dt_out, self.gauges, self.config, self.dx,
+                                rows=rows)
+            res = ens.run()
+            out.append(res.gauges)
+            self.last_ensemble = res
+            del ens
+        return torch.cat(out)
+
+
 def make_runup_problem(cases: int = 4, seed: int = 0, ny: int = 122, nx: int = 196,
                        dx: float = 0.028, duration: float = 22.5, dt_out: float = 0.1,
                        n_controls: int = 16, n_gauges: int = 6, device="cuda",
                        bathy_perturb: float = 0.01):
-    """Config 3 at a chosen resolution: the runup bathymetry (each case with
-    its own seeded Gaussian perturbation of the bed), walls except the west
-    water level, Manning n = 0.01, still water at rest, 16-control spline over
-    `duration` seconds sampled every `dt_out`, `n_gauges` seeded gauge cells
-    in the wet part.  Returns (problem, true raw controls [cases, n_controls])."""
-    from . import scenarios
-    from .config import SWEConfig
-    from .solver import SWE2D
+    """Config 3 at a chosen resolution (a RunupFamily): `cases` perturbed beds
+    and seeded true controls.  Returns (problem, true raw controls
+    [cases, n_controls])."""
+    fam = RunupFamily(ny, nx, dx, seed, duration, dt_out, n_controls, n_gauges, bathy_perturb,
+                      str(device))
     rng = np.random.default_rng(seed)
-    base = scenarios.runup(ny=ny, nx=nx, dx=dx, seed=seed)
-    beds = []
-    for c in range(cases):
-        z = base.bed.astype(np.float64).copy()
-        if bathy_perturb > 0:
-            X, Y = np.meshgrid((np.arange(nx) + 0.5) * dx, (np.arange(ny) + 0.5) * dx)
-            for _ in range(3):
-                cx, cy = rng.uniform(0.1, 0.9) * nx * dx, rng.uniform(0.1, 0.9) * ny * dx
-                amp = rng.uniform(-bathy_perturb, bathy_perturb)
-                sig = rng.uniform(0.05, 0.2)
-                z += amp * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * sig ** 2))
-        beds.append(z.astype(np.float32))
-    bed = torch.tensor(np.stack(beds)[:, None], device=device)
-    n = torch.full_like(bed, 0.01)
-    cfg = SWEConfig(**base.config)
-    model = SWE2D(bed, n, dx, dx, config=cfg, train_dem=False)
-    h0 = torch.clamp(-bed, min=0.0)
-    U0 = torch.cat([h0, torch.zeros_like(h0), torch.zeros_like(h0)], dim=1).contiguous()
-    wet = np.argwhere(np.stack(beds).max(0) < -0.03)
-    pick = rng.choice(len(wet), size=n_gauges, replace=False)
-    gauges = [tuple(int(v) for v in wet[i]) for i in pick]
-    n_out = int(round(duration / dt_out))
-    times = torch.arange(n_out, dtype=torch.float64) * dt_out
-    basis, _, _ = clamped_bspline_basis(times, n_controls, 3)
-    problem = InversionProblem(model, U0, gauges, dt_out, n_out, basis.float().to(device))
-    truth = torch.tensor(rng.uniform(-0.012, 0.015, size=(cases, n_controls)), dtype=torch.float32,
-                         device=device)
-    raw_true = raw_from_controls(truth)
-    with torch.no_grad():
-        problem.targets = problem.simulate(problem.series(raw_true), differentiable=False)
-    return problem, raw_true
+    beds = fam.beds(cases, rng)
+    truth = fam.controls(cases, rng)
+    problem = fam.problem(beds, truth)
+    return problem, raw_from_controls(torch.as_tensor(truth, device=device))
 
 
 __all__ = ["clamped_bspline_basis", "bounded_controls", "raw_from_controls", "InversionProblem",
-           "InversionResult", "invert", "gauge_rmse", "make_runup_problem", "math"]
+           "InversionResult", "invert", "gauge_rmse", "make_runup_problem", "RunupFamily", "math"]

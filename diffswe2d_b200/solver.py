@@ -527,9 +527,11 @@ class _DeviceLoop:
         self.clock.copy_(self.clock_host, non_blocking=True)
         self._clock_tick(self.bufs[0])  # sets up the first step
         if self.graph is None:
+            from .autotune import sweep_rows, tuned_rows_for_shape
             nat.load_kernels()
+            rows = tuned_rows_for_shape(self.B, self.ny, self.nx, self.dev)
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph):
+            with sweep_rows(rows), torch.cuda.graph(graph):
                 for s in range(self.chunk):
                     self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
             self.graph = graph

@@ -35,6 +35,7 @@ extern "C" {
 #define SWE_S_NONFINITE_STATE 1u /* NaN/Inf in the state read by a step */
 #define SWE_S_NONFINITE_DT 2u    /* non-finite CFL time step */
 #define SWE_S_NONPOSITIVE_DT 4u  /* time step <= 0 */
+#define SWE_S_STEP_LIMIT 8u      /* ensemble member in interval mode reached its step cap */
 
 /* Boundary codes (src/boundary.py:11-18). */
 #define SWE_BC_TRANSMISSIVE 0
@@ -156,6 +157,85 @@ int swe_clock_f32(swe_clock* clock, uint32_t* red, const float* series_t, const 
                   void* stream);
 
 /*
+ * Clock of a gauge run: n_out output intervals of out_dt seconds, each run
+ * exactly like one forward(U, t_end=out_dt, boundary_level=levels[c]) call
+ * (the per-chunk model run of the reference's inversion script,
+ * Examples/inverse/Monai_Valley/Monai_Velley_BC_inversion_spline_lr002/
+ * bc_inversion_train.py:332-411), with the gauges read after the last step
+ * of every interval.  base is what the clocked step kernels read; the host
+ * fills base.duration = out_dt, base.tolerance, base.max_dt_cap,
+ * base.max_steps (per interval), out_dt, n_out and record_cap, and zeroes
+ * the rest.
+ *
+ * Replay mode (replay = 1): the clock re-runs recorded steps
+ * [base.steps, replay_end) of an earlier run, each with its recorded dt as
+ * max_dt and its interval's level, so the recomputed states are the
+ * original ones bit for bit (the CFL dt of the same state is the same
+ * float, and min(cfl, dt) = dt).
+ */
+typedef struct swe_run_clock {
+    swe_clock base;
+    double out_dt;
+    int32_t n_out;
+    int32_t chunk;       /* current interval */
+    int32_t chunk_steps; /* steps taken in the current interval */
+    int32_t record_cap;  /* capacity of step_dt / step_code */
+    int32_t replay;      /* 1: replay recorded steps */
+    int32_t replay_end;  /* replay: one past the last step to re-run */
+} swe_run_clock;
+
+#define SWE_CLOCK_RECORD_FULL 4 /* more steps than record_cap: nothing recorded past it */
+
+/*
+ * swe_run_clock_f32: the bookkeeping between two steps of a gauge run.
+ * Run mode: after a step, elapsed += dt (with the end-of-call clamp of
+ * solver.py:766-768) and the step is recorded as step_dt[s] = dt,
+ * step_code[s] = 2*interval + (1 if the step ends its interval); at the end
+ * of an interval gauge_out[(b*n_out + c)*ngauge + g] = h + bed at gauge cell
+ * (gauge_cells[2g], gauge_cells[2g+1]) of U (the state after the step) for
+ * every batch member b, and the next interval starts (elapsed = 0).  Then
+ * the next step is set up as swe_clock_f32 does, with the interval's level
+ * levels[c*levelB + b] copied into level_out[levelB].  Replay mode: as
+ * described at swe_run_clock.  One block; no host synchronisation.
+ */
+int swe_run_clock_f32(swe_run_clock* clock, uint32_t* red, const float* levels, int levelB,
+                      float* level_out, const float* U, const float* bed, int bedB, int B, int ny,
+                      int nx, const int32_t* gauge_cells, int ngauge, float* gauge_out,
+                      float* step_dt, int32_t* step_code, void* stream);
+
+/*
+ * Adjoint of the gauge reads of interval c: lam[b,0,gy,gx] +=
+ * g_gauge[(b*n_out + c)*ngauge + g] for every batch member and gauge (the
+ * bed term of eta = h + bed is not differentiated).  Gauge cells may
+ * repeat.  One block.
+ */
+int swe_gauge_adjoint_f32(float* lam, int B, int ny, int nx, const int32_t* gauge_cells,
+                          int ngauge, const float* g_gauge, int n_out, int c, void* stream);
+
+/*
+ * Per-step setup of a device-driven gauge-run backward pass, so a segment of
+ * adjoint steps can be captured in one CUDA graph: with s = *cursor,
+ * code = step_code[s], c = code >> 1: dt_out[0] = step_dt[s],
+ * level_out[b] = levels[c*levelB + b], and if code & 1 (step s ended
+ * interval c) the gauge adjoint of swe_gauge_adjoint_f32 is added to lam.
+ * A cursor outside [0, nsteps) (the recorded steps) does nothing.  One block.
+ */
+int swe_gauge_adjoint_prep_f32(const int32_t* cursor, const float* step_dt,
+                               const int32_t* step_code, const float* levels, int levelB,
+                               float* dt_out, float* level_out, float* lam, int B, int ny, int nx,
+                               const int32_t* gauge_cells, int ngauge, const float* g_gauge,
+                               int n_out, int nsteps, void* stream);
+
+/*
+ * Per-step finish: g_levels[c*levelB + b] += the sum over nparts and blocks
+ * of parts[(part*B + b)*blocks + k] (summed over b as well when levelB = 1),
+ * c the interval of step *cursor; then *cursor -= 1.  One block.
+ */
+int swe_gauge_adjoint_post_f32(int32_t* cursor, const int32_t* step_code, const float* parts,
+                               int nparts, int B, int blocks, int levelB, float* g_levels,
+                               int nsteps, void* stream);
+
+/*
  * One stage (1, 2 or 3 = both) of a step driven by a device clock: like
  * swe_step_stage_f32 but max_dt comes from clock->max_dt and a step whose
  * clock is not active does nothing except copy U to U_out in stage 2.  The
@@ -200,6 +280,13 @@ int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float*
                           int ny, int nx, const swe_params* p, float dt, const float* lam_out,
                           float* lam_U, float* lam_k, float* lam_n, float* P_out, void* stream);
 
+/* swe_adj_pointwise_f32 with the time step read from device memory
+ * (*dt_dev), for launches captured in a CUDA graph whose step varies. */
+int swe_adj_pointwise_dev_f32(int mode, const float* U, const float* k, const float* n, int nB,
+                              int B, int ny, int nx, const swe_params* p, const float* dt_dev,
+                              const float* lam_out, float* lam_U, float* lam_k, float* lam_n,
+                              float* P_out, void* stream);
+
 /* ---------------------------------------------------------------------
  * Ensembles: many independent scenarios in one persistent launch.
  * (No counterpart in the reference, whose batch dimension requires equal
@@ -209,7 +296,15 @@ int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float*
 /* One scenario: its own grid, bed, roughness, configuration, boundary level
  * (constant or a series) and step count; every time step is its own CFL
  * step (capped by max_dt).  Device pointers; the state starts in U_a and
- * after `steps` steps is in U_a (even steps) or U_b (odd). */
+ * after `steps` steps is in U_a (even steps) or U_b (odd).
+ *
+ * Interval mode (n_out > 0): the member runs n_out output intervals of
+ * out_dt seconds exactly as swe_run_clock_f32 does (each interval like one
+ * forward(t_end=out_dt) call with level out_levels[c]; max_dt, if > 0, caps
+ * each step), writes eta = h + bed at its gauge cells after every interval
+ * into gauge_out[c*ngauge + g], and stops after the last interval; `steps`
+ * is then a cap (reaching it first fails the member with SWE_S_STEP_LIMIT);
+ * nseries and level are ignored. */
 typedef struct swe_ensemble_member {
     const float* bed;       /* [ny,nx] */
     const float* n;         /* [ny,nx] Manning n or roughness length */
@@ -227,7 +322,15 @@ typedef struct swe_ensemble_member {
     double start_time;      /* absolute time of the initial state */
     double max_dt;          /* cap on each step (float32-rounded) */
     swe_params params;      /* all members share apply_friction / friction_model */
+    double out_dt;          /* interval mode: seconds per output interval */
+    int32_t n_out;          /* interval mode: intervals (0: step-count mode) */
+    int32_t ngauge;         /* gauge cells */
+    const float* out_levels;     /* [n_out] boundary level of each interval */
+    const int32_t* gauge_cells;  /* [2*ngauge] (row, column) */
+    float* gauge_out;            /* [n_out*ngauge] eta after each interval */
 } swe_ensemble_member;
+
+#define SWE_ENSEMBLE_MAX_GAUGES 64
 
 typedef struct swe_ensemble_result {
     int32_t steps;     /* steps completed */
@@ -269,6 +372,10 @@ int swe_load_kernels(void);
 /* Output rows per tile of the single-grid sweep kernels (process-wide
  * tuning knob, default 64; set it between launches, not during them). */
 int swe_tune_sweep_rows(int rows);
+
+/* The current value of that knob (CUDA graphs keep the value they were
+ * captured with). */
+int swe_sweep_rows(void);
 
 /*
  * swe_step_noalloc_f32 -- one step like swe_step_f32, for callers that must

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from diffswe2d_b200 import SWE2D, SWEConfig, scenarios
-from diffswe2d_b200.autotune import size_class, tuned_rows
+from diffswe2d_b200.autotune import ROW_CHOICES, size_class, tuned_rows
 from diffswe2d_b200.ensemble import Ensemble
 
 pytestmark = pytest.mark.gpu
@@ -62,4 +62,35 @@ def test_ensemble_matches_each_scenario_alone(rows):
 
 def test_size_classes_and_default_rows():
     assert size_class(1000) == 0 and size_class(1 << 17) == 1 and size_class(1 << 30) == 3
-    assert tuned_rows(96 * 96, DEV) in (16, 32, 64, 128)
+    assert tuned_rows(96 * 96, DEV) in ROW_CHOICES
+
+
+def test_gauge_ensemble_matches_gauge_run_per_member():
+    """Interval mode: each member's gauges and final state are bit for bit
+    those of gauge_run on that member alone (its own CFL steps)."""
+    from diffswe2d_b200.ensemble import GaugeEnsemble
+    from diffswe2d_b200.gauge_run import gauge_run
+    sc = scenarios.runup(ny=61, nx=98, dx=0.056, seed=5)
+    cfg = SWEConfig(**sc.config)
+    M, n_out, out_dt = 3, 9, 0.3
+    base = torch.from_numpy(sc.bed).to(DEV)
+    bed = torch.stack([base + 0.003 * m for m in range(M)]).contiguous()
+    h0 = torch.clamp(-bed, min=0.0)
+    U0 = torch.stack([h0, torch.zeros_like(h0), torch.zeros_like(h0)], dim=1).contiguous()
+    t = torch.arange(n_out, device=DEV, dtype=torch.float32)
+    levels = torch.stack([0.01 * torch.sin(0.5 * t + m) for m in range(M)]).contiguous()
+    gauges = [(10, 20), (30, 40), (50, 10)]
+    n = torch.from_numpy(sc.roughness).to(DEV)[None]
+    ens = GaugeEnsemble(bed, n, U0, levels, out_dt, gauges, cfg, sc.dx)
+    res = ens.run()
+    for m in range(M):
+        model = SWE2D(bed[m], n[0], sc.dx, sc.dy, config=cfg, train_dem=False)
+        with torch.no_grad():
+            g, U = gauge_run(model, U0[m:m + 1], levels[m], out_dt, gauges)
+        assert torch.equal(res.gauges[m], g[0]), f"member {m}"
+        assert torch.equal(res.states[m], U[0])
+    res2 = ens.run()
+    assert torch.equal(res.gauges, res2.gauges)
+    capped = GaugeEnsemble(bed, n, U0, levels, out_dt, gauges, cfg, sc.dx, max_steps=5)
+    with pytest.raises(RuntimeError, match="step cap"):
+        capped.run()
