@@ -53,11 +53,22 @@ def parse():
     ap.add_argument("--nx", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["runup4096", "ensemble"], default="runup4096",
+    ap.add_argument("--workload", choices=["runup4096", "ensemble", "inversion", "warmstart"],
+                    default="runup4096",
                     help="runup4096: the headline single-grid step; ensemble: 64 scenarios of "
                          "uneven sizes in one persistent launch vs 64 sequential runs")
     ap.add_argument("--ensemble-steps", type=int, default=2000)
     ap.add_argument("--ensemble-count", type=int, default=64)
+    ap.add_argument("--inv-cases", type=int, default=4,
+                    help="inversion: runup cases inverted together")
+    ap.add_argument("--inv-grid", default="244x393x0.014", help="inversion: ny x nx x dx")
+    ap.add_argument("--inv-duration", type=float, default=22.5, help="inversion: seconds simulated")
+    ap.add_argument("--ws-train", type=int, default=20000, help="warmstart: training runs")
+    ap.add_argument("--ws-cases", type=int, default=100, help="warmstart: held-out cases")
+    ap.add_argument("--ws-max-iters", type=int, default=300)
+    ap.add_argument("--ws-epochs", type=int, default=30)
+    ap.add_argument("--ws-grid", default="61x98x0.056",
+                    help="warmstart: ny x nx x dx of the runup family")
     return ap.parse_args()
 
 
@@ -297,11 +308,131 @@ def run_ensemble(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_inversion(args, world, rank, local):
+    """Config 3: boundary-inflow inversion on the runup grid (default 244 x
+    393, dx 0.014 m; 16 controls, 6 gauges every 0.02 s over 22.5 s, Adam lr
+    0.002): time per Adam iteration (one gauge run forward + its checkpointed
+    adjoint) for `--inv-cases` cases inverted together.  A step of the metric
+    is one iteration; cell-updates count forward steps only."""
+    from diffswe2d_b200.inversion import make_runup_problem
+    from diffswe2d_b200.gauge_run import _WORKSPACES
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    gy, gx, gdx = args.inv_grid.split("x")
+    gy, gx, gdx = int(gy), int(gx), float(gdx)
+    problem, raw_true = make_runup_problem(cases=args.inv_cases, seed=0, ny=gy, nx=gx, dx=gdx,
+                                           duration=args.inv_duration, dt_out=0.02, device=dev)
+    raw = torch.zeros_like(raw_true).requires_grad_(True)
+    opt = torch.optim.Adam([raw], lr=0.002)
+    clk = Clocks(local)
+
+    def iteration():
+        opt.zero_grad(set_to_none=True)
+        sim = problem.simulate(problem.series(raw))
+        loss = ((sim - problem.targets) ** 2).mean(dim=(1, 2)).sum()
+        loss.backward()
+        opt.step()
+        return loss
+
+    for _ in range(max(args.warmup, 1)):
+        iteration()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clk:
+        e0.record()
+        for _ in range(args.steps):
+            loss = iteration()
+        e1.record()
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    steps = [w.last_steps for w in _WORKSPACES.values()][0]
+    cells = args.inv_cases * gy * gx * steps
+    line = {
+        "metric": "adjoint inversion: seconds per Adam iteration (config 3)",
+        "value": ms / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"runup_inversion_{gy}x{gx}", "dx": gdx, "cases": args.inv_cases,
+                   "controls": 16, "gauges": 6, "dt_out": 0.02, "duration_s": args.inv_duration,
+                   "lr": 0.002,
+                   "solver_steps_per_run": steps, "checkpoint_every": 128,
+                   "l2": "per-iteration working set (states, checkpoints, face buffers) > L2"},
+        "forward_plus_adjoint_mcell_per_s": cells / (ms * 1e-3) / 1e6,
+        "loss": float(loss), "clocks": clk.summary(),
+        "gpu_launches": steps * 21 * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_warmstart(args, world, rank, local):
+    """Config 5 at a reduced grid: learned warm start + adjoint inversion
+    against the plain (cold-start) inversion, both Adam lr 0.002 until each
+    held-out case's gauge RMSE <= 1e-4 m.  Training runs come from the
+    persistent ensemble kernel; the network is trained by the project's own
+    kernels.  value = median wall time to tolerance of the warm-started
+    cases (inference included)."""
+    from diffswe2d_b200.inversion import RunupFamily
+    from diffswe2d_b200.warmstart import WarmStartNet
+    from diffswe2d_b200.warmstart_study import compare, generate, train
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ny, nx, dx = args.ws_grid.split("x")
+    fam = RunupFamily(int(ny), int(nx), float(dx), seed=0, device=str(dev))
+    clk = Clocks(local)
+    with clk:
+        data = generate(fam, args.ws_train, seed=1)
+        net = WarmStartNet(dev, seed=0)
+        log = train(net, data, epochs=args.ws_epochs, batch=256, lr=2e-3)
+        res = compare(fam, net, cases=args.ws_cases, seed=12345, max_iters=args.ws_max_iters,
+                      tol=1e-4)
+    warm_t = [t for t in res["warm"]["seconds_to_tol"] if t is not None]
+    cold_t = [t for t in res["cold"]["seconds_to_tol"] if t is not None]
+    line = {
+        "metric": "inversion wall-time to gauge RMSE <= 1e-4 m (learned warm start)",
+        "value": float(np.median(warm_t)) if warm_t else None, "unit": "s", "n_gpus": 1,
+        "steps": res["warm"]["median_iterations"], "warmup": 0,
+        "ms_per_step": res["warm"]["seconds_per_iteration"] * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 solver and adjoint; bf16 products with fp32 accumulation in the network",
+        "data": "synthetic (solver-generated runs)",
+        "config": {"workload": f"runup_warmstart_{ny}x{nx}", "dx": float(dx), "training_runs": args.ws_train,
+                   "held_out_cases": args.ws_cases, "tol_m": 1e-4, "lr": 0.002,
+                   "max_iters": args.ws_max_iters, "samples": 1125, "gauges": 6, "controls": 16},
+        "warm": {"reached": res["warm"]["reached"], "median_iterations": res["warm"]["median_iterations"],
+                 "median_seconds_to_tol": float(np.median(warm_t)) if warm_t else None,
+                 "seconds_per_iteration": res["warm"]["seconds_per_iteration"],
+                 "median_initial_rmse": float(np.median(res["warm"]["initial_rmse"])),
+                 "inference_s": res["inference_s"]},
+        "cold": {"reached": res["cold"]["reached"], "median_iterations": res["cold"]["median_iterations"],
+                 "median_seconds_to_tol": float(np.median(cold_t)) if cold_t else None,
+                 "wall_seconds_at_cap": res["cold"]["wall_seconds"],
+                 "median_initial_rmse": float(np.median(res["cold"]["initial_rmse"])),
+                 "median_final_rmse": float(np.median(res["cold"]["final_rmse"]))},
+        "predicted_control_rmse_m": res["pred_control_rmse_m"],
+        "training": {"runs": args.ws_train, "generation_s": data.seconds,
+                     "generation_mcell_per_s": data.cell_updates / data.seconds / 1e6,
+                     "epochs": log.epochs, "steps": log.steps, "train_s": log.seconds,
+                     "val_control_rmse_m": log.val_rmse_m},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.workload == "ensemble" and args.impl == "b200":
         run_ensemble(args, world, rank, local)
+        return
+    if args.workload in ("inversion", "warmstart") and args.impl == "b200":
+        if rank == 0:
+            (run_inversion if args.workload == "inversion" else run_warmstart)(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

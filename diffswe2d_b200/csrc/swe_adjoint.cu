@@ -86,7 +86,7 @@ __device__ PrimRec padded_prim(const AdjArgs& a, int b, int j, int i) {
         const float hr = fmaxf(lev - z, 0.0f);
         const float hg = U0;
         const float hc = hr > a.kc.absorb_lim ? hr : hg;
-        const float c = sqrtf(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
+        const float c = root(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
         const float val = ((side == 0 || side == 2) ? -c : c) * (hg - hr);
         if (xarm) U1 = val;
         else U2 = val;
@@ -117,19 +117,20 @@ __global__ void adj_face_kernel(const AdjArgs a) {
         // adjoints of the face outputs from the tendencies of the two cells
         // sharing the face: (F_right(f) - F_left(f+1)) / d
         const float d = DIRY ? a.kc.dy : a.kc.dx;
+        const float rd = DIRY ? a.kc.rdy : a.kc.rdx;  // RN(1/d): lrhs / d below is exact RN
         const int n = DIRY ? ny : nx;
         float r0p = 0.0f, r1p = 0.0f, r2p = 0.0f, r0m = 0.0f, r1m = 0.0f, r2m = 0.0f;
         if (f < n) {  // cell f: this face is its left/top face
             const size_t o = DIRY ? a3(b, 0, f, row, ny, nx) : a3(b, 0, row, f, ny, nx);
-            r0p = a.lrhs[o] / d;
-            r1p = a.lrhs[o + plane] / d;
-            r2p = a.lrhs[o + 2 * plane] / d;
+            r0p = quot(a.lrhs[o], d, rd);
+            r1p = quot(a.lrhs[o + plane], d, rd);
+            r2p = quot(a.lrhs[o + 2 * plane], d, rd);
         }
         if (f >= 1) {  // cell f-1: this face is its right/bottom face
             const size_t o = DIRY ? a3(b, 0, f - 1, row, ny, nx) : a3(b, 0, row, f - 1, ny, nx);
-            r0m = a.lrhs[o] / d;
-            r1m = a.lrhs[o + plane] / d;
-            r2m = a.lrhs[o + 2 * plane] / d;
+            r0m = quot(a.lrhs[o], d, rd);
+            r1m = quot(a.lrhs[o + plane], d, rd);
+            r2m = quot(a.lrhs[o + 2 * plane], d, rd);
         }
         const float l_mass = r0p - r0m;
         // x: channel 1 normal, 2 tangential; y: channel 1 tangential, 2 normal
@@ -234,13 +235,16 @@ __device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float
             const bool use_hr = hr > a.kc.absorb_lim;
             const float hc = use_hr ? hr : hg;
             const float cm = fmaxf(hc, a.kc.absorb_min);
-            const float c = sqrtf(a.kc.g981 * cm);
+            const float c = root(a.kc.g981 * cm);
             const float s = (side == 0 || side == 2) ? -1.0f : 1.0f;
             const float lv = lg[normal];
             const float l_c = lv * (s * (hg - hr));
             const float l_diff = lv * (s * c);
             float l_hc = 0.0f;
-            if (hc >= a.kc.absorb_min) l_hc = a.kc.g981 * (l_c / (2.0f * c));
+            if (hc >= a.kc.absorb_min) {
+                const float c2 = 2.0f * c;
+                l_hc = a.kc.g981 * quot(l_c, c2, shared_rcp(c2));
+            }
             float l_hg = l_diff + (use_hr ? 0.0f : l_hc);
             float l_hr = -l_diff + (use_hr ? l_hc : 0.0f);
             lam[0] += l_hg;

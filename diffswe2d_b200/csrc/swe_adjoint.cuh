@@ -74,6 +74,7 @@ SWE_HD void incr_bwd(const Incr& r, float lam, float theta, float& lqm, float& l
 struct PrimRec {
     float U0, U1, U2, z;
     float h, safe, u, v, eta;
+    float rsafe;  // shared_rcp(safe): every quotient by safe uses it
     bool wet;
 };
 
@@ -86,8 +87,9 @@ SWE_HD PrimRec prim_rec(float U0, float U1, float U2, float z, const SweConsts& 
     p.h = fmaxf(U0, 0.0f);
     p.wet = p.h > k.dry;
     p.safe = fmaxf(p.h, k.floor_h);
-    p.u = p.wet ? U1 / p.safe : 0.0f;
-    p.v = p.wet ? U2 / p.safe : 0.0f;
+    p.rsafe = shared_rcp(p.safe);
+    p.u = p.wet ? quot(U1, p.safe, p.rsafe) : 0.0f;
+    p.v = p.wet ? quot(U2, p.safe, p.rsafe) : 0.0f;
     p.eta = p.h + z;
     return p;
 }
@@ -99,9 +101,9 @@ SWE_HD void prim_bwd(const PrimRec& p, float lh, float lsafe, float lu, float lv
                      const SweConsts& k, float& lU0, float& lU1, float& lU2) {
     lh += leta;
     if (p.wet) {
-        lU1 += lu / p.safe;
-        lU2 += lv / p.safe;
-        lsafe -= lu * (p.u / p.safe) + lv * (p.v / p.safe);
+        lU1 += quot(lu, p.safe, p.rsafe);
+        lU2 += quot(lv, p.safe, p.rsafe);
+        lsafe -= lu * quot(p.u, p.safe, p.rsafe) + lv * quot(p.v, p.safe, p.rsafe);
     }
     if (p.h >= k.floor_h) lh += lsafe;
     if (p.U0 >= 0.0f) lU0 += lh;
@@ -136,7 +138,7 @@ SWE_HD SideRec side_fwd(const PrimRec& a, const PrimRec& c, const PrimRec& b, bo
         if (r.reset) deta = dh + dz;
     }
     const float hdh = 0.5f * dh;
-    r.q = hdh / c.safe;
+    r.q = quot(hdh, c.safe, c.rsafe);
     if (plus) {
         r.s.hlin = c.h + hdh;
         r.s.eta = c.eta + 0.5f * deta;
@@ -181,8 +183,8 @@ SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin
     float l_fraw = (r.f_raw >= -10.0f && r.f_raw <= 10.0f) ? l_f : 0.0f;
     float l_q = c.h > k.dry ? -sg * l_fraw : 0.0f;
     // q = (0.5 dh) / safe
-    float l_dh = 0.5f * (l_q / c.safe);
-    lc.safe -= l_q * (r.q / c.safe);
+    float l_dh = 0.5f * quot(l_q, c.safe, c.rsafe);
+    lc.safe -= l_q * quot(r.q, c.safe, c.rsafe);
     // hlin = h +/- 0.5 dh ; eta_side = eta +/- 0.5 deta
     lc.h += l_hlin;
     l_dh += sg * (0.5f * l_hlin);
@@ -227,9 +229,10 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     const float hL = fmaxf(hcL, 0.0f), hR = fmaxf(hcR, 0.0f);
     const bool wetL = hL > k.dry, wetR = hR > k.dry;
     const float safeL = fmaxf(hL, k.floor_h), safeR = fmaxf(hR, k.floor_h);
-    const float uL = wetL ? UL1 / safeL : 0.0f, vL = wetL ? UL2 / safeL : 0.0f;
-    const float uR = wetR ? UR1 / safeR : 0.0f, vR = wetR ? UR2 / safeR : 0.0f;
-    const float cL = wetL ? sqrtf(k.g * safeL) : 0.0f, cR = wetR ? sqrtf(k.g * safeR) : 0.0f;
+    const float ysL = shared_rcp(safeL), ysR = shared_rcp(safeR);
+    const float uL = wetL ? quot(UL1, safeL, ysL) : 0.0f, vL = wetL ? quot(UL2, safeL, ysL) : 0.0f;
+    const float uR = wetR ? quot(UR1, safeR, ysR) : 0.0f, vR = wetR ? quot(UR2, safeR, ysR) : 0.0f;
+    const float cL = wetL ? root(k.g * safeL) : 0.0f, cR = wetR ? root(k.g * safeR) : 0.0f;
     const float unL = normal_y ? vL : uL, utL = normal_y ? uL : vL;
     const float unR = normal_y ? vR : uR, utR = normal_y ? uR : vR;
     const float us = (0.5f * (unL + unR) + cL) - cR;
@@ -248,7 +251,8 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     const float numh = (SR * fhL - SL * fhR) + SLSR * (hR - hL);
     const float mom = hR * unR - hL * unL;
     const float numq = (SR * fqL - SL * fqR) + SLSR * mom;
-    const float fhs = numh / den, fqs = numq / den;
+    const float yden = shared_rcp(den);
+    const float fhs = quot(numh, den, yden), fqs = quot(numq, den, yden);
     const bool lf = SL >= 0.0f, rf = SR <= 0.0f;
     const float fh = lf ? fhL : (rf ? fhR : fhs);
     const bool both = ldry && rdry;
@@ -278,8 +282,8 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
         l_fqs = l_fq;
     }
     // fhs = numh / den, fqs = numq / den
-    const float l_numh = l_fhs / den, l_numq = l_fqs / den;
-    const float l_den = -(l_fhs * (fhs / den)) - l_fqs * (fqs / den);
+    const float l_numh = quot(l_fhs, den, yden), l_numq = quot(l_fqs, den, yden);
+    const float l_den = -(l_fhs * quot(fhs, den, yden)) - l_fqs * quot(fqs, den, yden);
     float l_SL = 0.0f, l_SR = 0.0f, l_hL = 0.0f, l_hR = 0.0f, l_unL = 0.0f, l_unR = 0.0f;
     float l_cL = 0.0f, l_cR = 0.0f;
     // numh = (SR fhL - SL fhR) + SLSR (hR - hL)
@@ -360,16 +364,18 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     // primitive() of the face states
     float l_UL1 = 0.0f, l_UL2 = 0.0f, l_UR1 = 0.0f, l_UR2 = 0.0f, l_safeL = 0.0f, l_safeR = 0.0f;
     if (wetL) {
-        l_UL1 = l_uL / safeL;
-        l_UL2 = l_vL / safeL;
-        l_safeL -= l_uL * (uL / safeL) + l_vL * (vL / safeL);
-        l_safeL += k.g * (l_cL / (2.0f * cL));
+        l_UL1 = quot(l_uL, safeL, ysL);
+        l_UL2 = quot(l_vL, safeL, ysL);
+        l_safeL -= l_uL * quot(uL, safeL, ysL) + l_vL * quot(vL, safeL, ysL);
+        const float c2 = 2.0f * cL;
+        l_safeL += k.g * quot(l_cL, c2, shared_rcp(c2));
     }
     if (wetR) {
-        l_UR1 = l_uR / safeR;
-        l_UR2 = l_vR / safeR;
-        l_safeR -= l_uR * (uR / safeR) + l_vR * (vR / safeR);
-        l_safeR += k.g * (l_cR / (2.0f * cR));
+        l_UR1 = quot(l_uR, safeR, ysR);
+        l_UR2 = quot(l_vR, safeR, ysR);
+        l_safeR -= l_uR * quot(uR, safeR, ysR) + l_vR * quot(vR, safeR, ysR);
+        const float c2 = 2.0f * cR;
+        l_safeR += k.g * quot(l_cR, c2, shared_rcp(c2));
     }
     if (hL >= k.floor_h) l_hL += l_safeL;
     if (hR >= k.floor_h) l_hR += l_safeR;
