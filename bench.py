@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--ws-cases", type=int, default=100, help="warmstart: held-out cases")
     ap.add_argument("--ws-max-iters", type=int, default=300)
     ap.add_argument("--ws-epochs", type=int, default=30)
+    ap.add_argument("--ws-cold-lr2", type=float, default=0.0,
+                    help="warmstart: also run the cold start at this learning rate (0: no)")
     ap.add_argument("--ws-grid", default="61x98x0.056",
                     help="warmstart: ny x nx x dx of the runup family")
     return ap.parse_args()
@@ -385,7 +387,7 @@ def run_warmstart(args, world, rank, local):
         net = WarmStartNet(dev, seed=0)
         log = train(net, data, epochs=args.ws_epochs, batch=256, lr=2e-3)
         res = compare(fam, net, cases=args.ws_cases, seed=12345, max_iters=args.ws_max_iters,
-                      tol=1e-4)
+                      tol=1e-4, extra_cold_lrs=(args.ws_cold_lr2,) if args.ws_cold_lr2 > 0 else ())
     warm_t = [t for t in res["warm"]["seconds_to_tol"] if t is not None]
     cold_t = [t for t in res["cold"]["seconds_to_tol"] if t is not None]
     line = {
@@ -409,6 +411,13 @@ def run_warmstart(args, world, rank, local):
                  "wall_seconds_at_cap": res["cold"]["wall_seconds"],
                  "median_initial_rmse": float(np.median(res["cold"]["initial_rmse"])),
                  "median_final_rmse": float(np.median(res["cold"]["final_rmse"]))},
+        **{k: {"lr": float(k[len("cold_lr"):]), "reached": v["reached"],
+               "median_iterations": v["median_iterations"],
+               "median_seconds_to_tol": (float(np.median([t for t in v["seconds_to_tol"] if t is not None]))
+                                         if v["reached"] else None),
+               "wall_seconds_at_cap": v["wall_seconds"],
+               "median_final_rmse": float(np.median(v["final_rmse"]))}
+           for k, v in res.items() if k.startswith("cold_lr")},
         "predicted_control_rmse_m": res["pred_control_rmse_m"],
         "training": {"runs": args.ws_train, "generation_s": data.seconds,
                      "generation_mcell_per_s": data.cell_updates / data.seconds / 1e6,

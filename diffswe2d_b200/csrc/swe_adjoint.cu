@@ -323,14 +323,15 @@ struct PwArgs {
 __device__ void clean_bwd(const State& o, const State& c, const State& lout, const SweConsts& k,
                           bool positivity, State& lold, State& lcand) {
     State cp = c;
-    float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, th = 1.0f, ratio = 0.0f, safe = 0.0f;
+    float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, th = 1.0f, ratio = 0.0f, safe = 0.0f, ysafe = 0.0f;
     bool theta_branch = false;
     if (positivity) {
         d0 = c.h - o.h;
         d1 = c.hu - o.hu;
         d2 = c.hv - o.hv;
         safe = fmaxf(-d0, k.eps);
-        ratio = o.h / safe;
+        ysafe = shared_rcp(safe);
+        ratio = quot(o.h, safe, ysafe);
         theta_branch = d0 < 0.0f;
         th = theta_branch ? fminf(ratio, 1.0f) : 1.0f;
         cp.h = o.h + th * d0;
@@ -353,8 +354,8 @@ __device__ void clean_bwd(const State& o, const State& c, const State& lout, con
     float ld0 = lcp.h * th, ld1 = lcp.hu * th, ld2 = lcp.hv * th;
     lold = lcp;
     if (theta_branch && ratio <= 1.0f) {  // th = clamp(old_h / safe, max=1)
-        lold.h += l_th / safe;
-        const float l_safe = -l_th * (ratio / safe);
+        lold.h += quot(l_th, safe, ysafe);
+        const float l_safe = -l_th * quot(ratio, safe, ysafe);
         if (-d0 >= k.eps) ld0 -= l_safe;  // safe = clamp(-dh, min=eps)
     }
     lcand = State{ld0, ld1, ld2};
@@ -370,11 +371,12 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
     const float h = fmaxf(s0.h, 0.0f);
     const bool wet = h > k.dry;
     const float safe = fmaxf(h, k.fr_vs);
-    const float u = (wet ? s0.hu : 0.0f) / safe, v = (wet ? s0.hv : 0.0f) / safe;
+    const float ys = shared_rcp(safe);
+    const float u = quot(wet ? s0.hu : 0.0f, safe, ys), v = quot(wet ? s0.hv : 0.0f, safe, ys);
     const float sp2 = u * u + v * v;
     const bool moving = wet && sp2 > 0.0f;
     const float S = fmaxf(sp2, k.fr_e2);
-    const float speed = moving ? sqrtf(S) : 0.0f;
+    const float speed = moving ? root(S) : 0.0f;
     float cf;
     // cf and d cf / d h, d cf / d n (as autograd evaluates them)
     float dcf_dpre = 0.0f, dcf_dn = 0.0f, hpre = 0.0f;
@@ -384,63 +386,66 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
         hpre = fmaxf(h, k.fr_e);
         const float pw = pow_third(hpre, k.third);
         const float num = k.g981 * (nn * nn);
-        cf = num / pw;
+        const float ypw = shared_rcp(pw);
+        cf = quot(num, pw, ypw);
         // d/d pw: -cf / pw ; d pw / d hpre = third * hpre^(third - 1)
         const float dpw = k.third * (float)pow((double)hpre, (double)(k.third - 1.0f));
-        dcf_dpre = -(cf / pw) * dpw;
-        dcf_dn = (k.g981 * (2.0f * nn)) / pw;
+        dcf_dpre = -quot(cf, pw, ypw) * dpw;
+        dcf_dn = quot(k.g981 * (2.0f * nn), pw, ypw);
         h_pass = h >= k.fr_e;
         n_pass = n >= 0.0f;
     } else {
         const float zz = fmaxf(n, k.fr_e);
         hpre = fmaxf(h, k.fr_e);
-        const float ratio = hpre / zz;
+        const float yzz = shared_rcp(zz);
+        const float ratio = quot(hpre, zz, yzz);
         const float shallow_den = fmaxf(0.46f * ratio, k.fr_e);
         const float rc = fmaxf(ratio, k.fr_e);
         const float lg = (float)log((double)rc);
-        const float inv_rc = 1.0f / rc;
+        const float inv_rc = recip(rc);
         const float lt = 2.5f * ((lg - 1.0f) + inv_rc * 1.359f);
         const float deep_den = fmaxf(lt * lt, k.fr_e);
         const bool shallow_b = ratio < 2.71828182845904523536f;
-        cf = shallow_b ? 1.0f / shallow_den : 1.0f / deep_den;
+        cf = shallow_b ? recip(shallow_den) : recip(deep_den);
         float dcf_dratio;
         if (shallow_b) {
             dcf_dratio = (0.46f * ratio >= k.fr_e) ? -(cf * cf) * 0.46f : 0.0f;
         } else {
             float dlt = 0.0f;
-            if (ratio >= k.fr_e) dlt = 2.5f * (1.0f / rc - 1.359f * inv_rc * inv_rc);
+            if (ratio >= k.fr_e) dlt = 2.5f * (inv_rc - 1.359f * inv_rc * inv_rc);
             dcf_dratio = (lt * lt >= k.fr_e) ? -(cf * cf) * (2.0f * lt) * dlt : 0.0f;
         }
-        dcf_dpre = dcf_dratio / zz;
-        dcf_dn = -dcf_dratio * (ratio / zz);
+        dcf_dpre = quot(dcf_dratio, zz, yzz);
+        dcf_dn = -dcf_dratio * quot(ratio, zz, yzz);
         h_pass = h >= k.fr_e;
         n_pass = n >= k.fr_e;
     }
-    const float X = ((cf * speed) * dt) / safe;
-    const float fac = 1.0f / (1.0f + X);
+    const float X = quot((cf * speed) * dt, safe, ys);
+    const float fac = recip(1.0f + X);
     ls.h = lout.h;
     ls.hu = wet ? lout.hu * fac : 0.0f;
     ls.hv = wet ? lout.hv * fac : 0.0f;
     float l_fac = wet ? lout.hu * s0.hu + lout.hv * s0.hv : 0.0f;
     const float l_D = -l_fac * (fac * fac);
-    const float l_num = l_D / safe;  // d/d((cf speed) dt)
-    float l_safe = -l_D * (X / safe);
+    const float l_num = quot(l_D, safe, ys);  // d/d((cf speed) dt)
+    float l_safe = -l_D * quot(X, safe, ys);
     const float l_cs = l_num * dt;
     const float l_cf = l_cs * speed;
     const float l_speed = l_cs * cf;
     float l_u = 0.0f, l_v = 0.0f;
     if (moving) {
-        const float l_S = l_speed / (2.0f * speed);
+        const float s2 = 2.0f * speed;
+        const float l_S = quot(l_speed, s2, shared_rcp(s2));
         if (sp2 >= k.fr_e2) {
             l_u = l_S * (2.0f * u);
             l_v = l_S * (2.0f * v);
         }
     }
     if (wet) {
-        ls.hu += l_u / safe;
-        ls.hv += l_v / safe;
+        ls.hu += quot(l_u, safe, ys);
+        ls.hv += quot(l_v, safe, ys);
     }
-    l_safe -= l_u * (u / safe) + l_v * (v / safe);
+    l_safe -= l_u * quot(u, safe, ys) + l_v * quot(v, safe, ys);
     float l_h = 0.0f;
     if (h >= k.fr_vs) l_h += l_safe;
     if (h_pass) l_h += l_cf * dcf_dpre;

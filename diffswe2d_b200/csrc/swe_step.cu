@@ -904,7 +904,9 @@ extern "C" int swe_spatial_operator_f32(const float* U, const float* bed, int B,
     a.red = red;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
-    stage_kernel<1><<<grid_of(a), NT, 0, s>>>(a);
+    // the stage-1 kernel of the step computes exactly this (tendency + maxima)
+    if (use_tiled_kernels()) stage_kernel<1><<<grid_of(a), NT, 0, s>>>(a);
+    else sweep_kernel<1, 0><<<sweep_grid_of(a), SW_WARPS * 32, 0, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 

@@ -238,6 +238,13 @@ class GaugeRunWorkspace:
         if self.lam_n is not None:
             self.lam_n.zero_()
         nseg = (total + self.k - 1) // self.k
+        from .autotune import sweep_rows
+        with sweep_rows(self.rows):
+            self._backward_segments(nseg, total)
+        lam_n = self.lam_n.clone() if self.lam_n is not None else None
+        return self.lam[0].clone(), self.g_levels.clone(), lam_n
+
+    def _backward_segments(self, nseg, total):
         for j in range(nseg - 1, -1, -1):
             s0, s1 = j * self.k, min((j + 1) * self.k, total)
             self._recompute_segment(j, s0, s1)
@@ -255,8 +262,6 @@ class GaugeRunWorkspace:
                 self.adj_graph = g
                 self.cursor.fill_(s1 - 1)  # the capture ran nothing; keep the cursor explicit
             self.adj_graph.replay()
-        lam_n = self.lam_n.clone() if self.lam_n is not None else None
-        return self.lam[0].clone(), self.g_levels.clone(), lam_n
 
 
 class _RecordFull(RuntimeError):

@@ -91,8 +91,10 @@ def train(net: WarmStartNet, data: Dataset, epochs: int = 30, batch: int = 256, 
 
 
 def compare(fam: RunupFamily, net: WarmStartNet, cases: int, seed: int, lr: float = 0.002,
-            max_iters: int = 400, tol: float = 1e-4) -> Dict:
-    """Cold and warm inversions of `cases` held-out cases (batched)."""
+            max_iters: int = 400, tol: float = 1e-4, extra_cold_lrs=()) -> Dict:
+    """Cold and warm inversions of `cases` held-out cases (batched), both
+    with Adam at `lr`; `extra_cold_lrs` adds cold-start runs at other
+    learning rates (e.g. 0.02, the inversion script's own setting)."""
     rng = np.random.default_rng(seed)
     beds = fam.beds(cases, rng)
     truth = fam.controls(cases, rng)
@@ -109,7 +111,12 @@ def compare(fam: RunupFamily, net: WarmStartNet, cases: int, seed: int, lr: floa
     t_inf = time.perf_counter() - t0
     res_warm = invert(problem, warm_raw, lr=lr, max_iters=max_iters, rmse_tol=tol)
     truth_t = torch.as_tensor(truth, device=pred.device)
+    extra = {}
+    for lr2 in extra_cold_lrs:
+        extra[f"cold_lr{lr2:g}"] = _summary(
+            invert(problem, cold_raw, lr=lr2, max_iters=max_iters, rmse_tol=tol), 0.0)
     return {
+        **extra,
         "cases": B,
         "tol_m": tol,
         "lr": lr,
