@@ -238,7 +238,8 @@ def run_ensemble(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     sizes = scenarios.ensemble_sizes(args.ensemble_count, seed=0)
-    mine = [(k, s) for k, s in enumerate(sizes) if k % world == rank]
+    from diffswe2d_b200.sharding import reduce_over_ranks, shard_indices
+    mine = [(k, sizes[k]) for k in shard_indices(len(sizes), world, rank)]
     members = []
     for k, (ny, nx) in mine:
         sc = scenarios.ensemble_member(ny, nx, seed=k)
@@ -279,14 +280,8 @@ def run_ensemble(args, world, rank, local):
         torch.cuda.synchronize(dev)
         seq_ms += e0.elapsed_time(e1)
     cells = res.cell_updates
-    if world > 1:
-        t = torch.tensor([ms, seq_ms, float(cells)], device=dev, dtype=torch.float64)
-        import torch.distributed as dist
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms, seq_ms, cells = float(mx[0]), float(mx[1]), int(sm[2])
+    ms, seq_ms = reduce_over_ranks([ms, seq_ms], "max", dev)
+    cells = int(reduce_over_ranks([cells], "sum", dev)[0])
     line = {
         "metric": "Mcell-updates/s (ensemble)", "value": cells / (ms * 1e-3) / 1e6,
         "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.ensemble_steps, "warmup": 1,
@@ -521,11 +516,8 @@ def main():
     total_ms = ev[0].elapsed_time(ev[-1])
     s1 = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
     s2 = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)]
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    from diffswe2d_b200.sharding import reduce_over_ranks
+    total_ms = reduce_over_ranks([total_ms], "max", dev)[0]  # max over ranks
     ms_per_step = total_ms / args.steps
     value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
     status = int(red[2].item())
@@ -556,11 +548,7 @@ def main():
             counts.append(model.last_forward_steps)
         e1.record()
         torch.cuda.synchronize(dev)
-        e2e_ms = e0.elapsed_time(e1)
-        if world > 1:
-            tt = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
+        e2e_ms = reduce_over_ranks([e0.elapsed_time(e1)], "max", dev)[0]
         nbytes = host_in.numel() * 4
         e2e = {"value": world * cells * sum(counts) / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,

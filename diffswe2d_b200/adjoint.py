@@ -15,8 +15,10 @@ detached as in ``src/solver.py:626``), wrapped in two autograd Functions:
   initial state; the backward pass recomputes the chunk's states (its
   checkpoint interval is the chunk) and runs the adjoint steps in reverse.
 
-Gradients flow to the state, the boundary level and the roughness field.
-The bed (``dem_correction_parameter``) is not differentiated.
+Gradients flow to the state, the boundary level, the roughness field and,
+when ``dem_correction_parameter`` requires grad, the bed (``model.bed`` is an
+autograd input, so the gradient reaches the correction parameter through
+the reference's ``tanh`` bound and valid mask, ``src/solver.py:134-147``).
 """
 from __future__ import annotations
 
@@ -27,11 +29,12 @@ from . import _native as nat
 LEVEL_BLOCKS = 64
 
 
-def _check_no_bed_grad(model):
+def bed_input(model):
+    """``model.bed`` as an autograd input when the DEM correction requires
+    grad (and autograd is on), else None."""
     if torch.is_grad_enabled() and model.dem_correction_parameter.requires_grad:
-        raise NotImplementedError(
-            "gradients with respect to the bed (dem_correction_parameter) are not provided by "
-            "the B200 adjoint; construct the model with train_dem=False")
+        return model.bed
+    return None
 
 
 class AdjointStepper:
@@ -39,16 +42,20 @@ class AdjointStepper:
     with their scratch buffers allocated once (a run's backward pass calls
     it once per step)."""
 
-    def __init__(self, model, B, ny, nx, dev, levelB, infiltration=None):
+    def __init__(self, model, B, ny, nx, dev, levelB, infiltration=None, bed_grad=False):
         shape = (B, 3, ny, nx)
         self.model = model
         self.B, self.ny, self.nx, self.levelB = B, ny, nx, levelB
+        self.bed_grad = bool(bed_grad)
+        rec = 16 if self.bed_grad else 12  # floats per face record
         self.K1, self.K2, self.P = (torch.empty(shape, device=dev) for _ in range(3))
         self.lam_k = torch.empty(shape, device=dev)
         self.lam_P = torch.empty(shape, device=dev)
         self.red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
-        self.cx = torch.empty(B * ny * (nx + 1) * 12, device=dev)
-        self.cy = torch.empty(B * (ny + 1) * nx * 12, device=dev)
+        self.cx = torch.empty(B * ny * (nx + 1) * rec, device=dev)
+        self.cy = torch.empty(B * (ny + 1) * nx * rec, device=dev)
+        # bed adjoint per batch member, accumulated over the steps of a pass
+        self.lam_bed = torch.zeros((B, ny, nx), device=dev) if self.bed_grad else None
         self.part = torch.empty((2, B * LEVEL_BLOCKS), device=dev)
         probe = torch.empty((B, 1, ny, nx), device=dev)
         self.bed, self.n = model._fields(probe.expand(B, 3, ny, nx))
@@ -56,7 +63,7 @@ class AdjointStepper:
         self.p = model._params()
         self.fric = bool(model.cfg.apply_friction)
         self.lib, self.dev = nat.lib(), dev
-        self.key = (B, ny, nx, str(dev), levelB)
+        self.key = (B, ny, nx, str(dev), levelB, self.bed_grad)
 
     @property
     def st(self):
@@ -70,6 +77,24 @@ class AdjointStepper:
             nat.ptr(lv), self.levelB, None, nat.FORCING_NONE, 1, nat.ptr(self.infil), self.imode,
             self.iB, nat.ptr(out), nat.ptr(self.red), self.st)
         nat.check(rc, "adjoint recompute")
+
+    def _spatial(self, S, lv, lam_rhs, lam_S, part, what):
+        args = (nat.ptr(S), nat.ptr(self.bed), self.bed.shape[0], self.B, self.ny, self.nx, self.p,
+                nat.ptr(lv), self.levelB, nat.ptr(lam_rhs), nat.ptr(self.cx), nat.ptr(self.cy),
+                nat.ptr(lam_S), nat.ptr(part), LEVEL_BLOCKS)
+        if self.bed_grad:
+            rc = self.lib.swe_adj_spatial_bed_f32(*args, nat.ptr(self.lam_bed), self.st)
+        else:
+            rc = self.lib.swe_adj_spatial_f32(*args, self.st)
+        nat.check(rc, what)
+
+    def bed_adjoint(self):
+        """The accumulated bed adjoint in the bed's batch form
+        [bedB, 1, ny, nx] (summed over the batch for a shared bed)."""
+        lb = self.lam_bed
+        if self.bed.shape[0] == 1:
+            lb = lb.sum(0, keepdim=True)
+        return lb.unsqueeze(1)
 
     def _pointwise(self, mode, U, k, dt, lam_out, lam_U, lam_n, P_out):
         n = self.n
@@ -104,19 +129,11 @@ class AdjointStepper:
         # corrector + friction
         self._pointwise(0, U, K2, dt, lam_out, lam_U, lam_n, None)
         # spatial operator at the predictor
-        rc = lib.swe_adj_spatial_f32(nat.ptr(P), nat.ptr(self.bed), self.bed.shape[0], B, ny, nx, p,
-                                     nat.ptr(lv), self.levelB, nat.ptr(lam_k), nat.ptr(self.cx),
-                                     nat.ptr(self.cy), nat.ptr(lam_P), nat.ptr(self.part[0]),
-                                     LEVEL_BLOCKS, st)
-        nat.check(rc, "adjoint spatial operator (stage 2)")
+        self._spatial(P, lv, lam_k, lam_P, self.part[0], "adjoint spatial operator (stage 2)")
         # predictor
         self._pointwise(1, U, K1, dt, lam_P, lam_U, None, None)
         # spatial operator at the input state
-        rc = lib.swe_adj_spatial_f32(nat.ptr(U), nat.ptr(self.bed), self.bed.shape[0], B, ny, nx, p,
-                                     nat.ptr(lv), self.levelB, nat.ptr(lam_k), nat.ptr(self.cx),
-                                     nat.ptr(self.cy), nat.ptr(lam_U), nat.ptr(self.part[1]),
-                                     LEVEL_BLOCKS, st)
-        nat.check(rc, "adjoint spatial operator (stage 1)")
+        self._spatial(U, lv, lam_k, lam_U, self.part[1], "adjoint spatial operator (stage 1)")
         return self.part
 
     def level_adjoint(self, part):
@@ -126,70 +143,80 @@ class AdjointStepper:
 
 
 def adjoint_step(model, U, level, n, dt, lam_out, infiltration=None, ws=None, lam_U=None,
-                 lam_n=None):
+                 lam_n=None, bed_grad=False):
     """VJP of one step at input state ``U`` with time step ``dt``.
 
-    Returns ``(lam_U, lam_level, lam_n)``: adjoints of the state
-    [B,3,ny,nx], the level vector (1 or B values) and the roughness field
-    (same shape as ``n``; None when friction is off).  ``ws`` is an optional
-    AdjointStepper built for the same model and shapes; ``lam_U`` / ``lam_n``
-    optional zeroed outputs that the step accumulates into.
+    Returns ``(lam_U, lam_level, lam_n, lam_bed)``: adjoints of the state
+    [B,3,ny,nx], the level vector (1 or B values), the roughness field (same
+    shape as ``n``; None when friction is off) and, with ``bed_grad``, the
+    bed ([bedB,1,ny,nx]; else None).  ``ws`` is an optional AdjointStepper
+    built for the same model and shapes; ``lam_U`` / ``lam_n`` optional
+    zeroed outputs that the step accumulates into.
     """
     U = nat.require_cuda_f32("U", U.detach())
     lam_out = nat.require_cuda_f32("lam_out", lam_out)
     B, _, ny, nx = U.shape
     dev = U.device
     lv, levelB = model._level_arg(level.detach(), B)
-    if ws is None or ws.key != (B, ny, nx, str(dev), levelB):
-        ws = AdjointStepper(model, B, ny, nx, dev, levelB, infiltration)
+    if ws is None or ws.key != (B, ny, nx, str(dev), levelB, bool(bed_grad)):
+        ws = AdjointStepper(model, B, ny, nx, dev, levelB, infiltration, bed_grad)
     lam_U = torch.zeros_like(U) if lam_U is None else lam_U
     if ws.fric and lam_n is None:
         lam_n = torch.zeros_like(ws.n)
+    if ws.bed_grad:
+        ws.lam_bed.zero_()
     part = ws(U, lv, dt, lam_out, lam_U, lam_n)
-    return lam_U, ws.level_adjoint(part), (lam_n if ws.fric else None)
+    lam_bed = ws.bed_adjoint() if ws.bed_grad else None
+    return lam_U, ws.level_adjoint(part), (lam_n if ws.fric else None), lam_bed
 
 
 class _StepFunction(torch.autograd.Function):
-    """One SWE2D.step as an autograd node (inputs: state, level vector, roughness)."""
+    """One SWE2D.step as an autograd node (inputs: state, level vector,
+    roughness, bed or None)."""
 
     @staticmethod
-    def forward(ctx, U, level_vec, n, model, max_dt_f, infiltration, dt_out):
+    def forward(ctx, U, level_vec, n, bed, model, max_dt_f, infiltration, dt_out):
         U_new, status, dt = model._launch_step(U.detach(), level_vec.detach(), max_dt_f, infiltration)
         model._raise_on_status(status, dt)
         dt_out.append(dt)
         ctx.model, ctx.dt, ctx.infiltration = model, dt, infiltration
+        ctx.bed_shape = None if bed is None else bed.shape
         ctx.save_for_backward(U, level_vec, n)
         return U_new
 
     @staticmethod
     def backward(ctx, gU):
         U, level_vec, n = ctx.saved_tensors
-        lam_U, lam_level, lam_n = adjoint_step(ctx.model, U, level_vec, n, ctx.dt, gU.contiguous(),
-                                               ctx.infiltration)
+        need_bed = ctx.bed_shape is not None and ctx.needs_input_grad[3]
+        lam_U, lam_level, lam_n, lam_bed = adjoint_step(ctx.model, U, level_vec, n, ctx.dt,
+                                                        gU.contiguous(), ctx.infiltration,
+                                                        bed_grad=need_bed)
         g_level = lam_level.reshape(level_vec.shape) if ctx.needs_input_grad[1] else None
         g_n = lam_n.reshape(n.shape) if (ctx.needs_input_grad[2] and lam_n is not None) else None
-        return lam_U, g_level, g_n, None, None, None, None
+        g_bed = lam_bed.reshape(ctx.bed_shape) if need_bed else None
+        return lam_U, g_level, g_n, g_bed, None, None, None, None
 
 
 def step_with_adjoint(model, U, model_time, max_dt, infiltration=None, boundary_level=None):
     """SWE2D.step under autograd: returns (U_new, dt_float) like the reference."""
-    _check_no_bed_grad(model)
     max_dt_f = float((max_dt.to(dtype=torch.float32) if torch.is_tensor(max_dt)
                       else torch.tensor(float(max_dt), dtype=torch.float32)).item())
     level = model._prepare_boundary_level(
         model.cfg.constant_level if boundary_level is None else boundary_level, U)
     level_vec = level.reshape(-1) if level.ndim > 0 else level.reshape(1)
     dt_out = []
-    U_new = _StepFunction.apply(U, level_vec, model.roughness_length, model, max_dt_f, infiltration,
-                                dt_out)
+    U_new = _StepFunction.apply(U, level_vec, model.roughness_length, bed_input(model), model,
+                                max_dt_f, infiltration, dt_out)
     return U_new, dt_out[0]
 
 
 class _ChunkFunction(torch.autograd.Function):
-    """A whole forward() call (explicit boundary level) as one autograd node."""
+    """A whole forward() call (explicit boundary level) as one autograd node
+    (inputs: initial state, level vector, roughness, bed or None)."""
 
     @staticmethod
-    def forward(ctx, U0, level_vec, n, model, t_end, start_time, max_dt_cap, max_steps, steps_out):
+    def forward(ctx, U0, level_vec, n, bed, model, t_end, start_time, max_dt_cap, max_steps,
+                steps_out):
         with torch.no_grad():
             U, _ = model.forward(U0.detach(), t_end=t_end, start_time=start_time,
                                  boundary_level=level_vec.detach(), max_dt_cap=max_dt_cap,
@@ -198,6 +225,7 @@ class _ChunkFunction(torch.autograd.Function):
         steps_out.append(steps)
         ctx.model, ctx.t_end, ctx.max_dt_cap, ctx.max_steps = model, t_end, max_dt_cap, max_steps
         ctx.start_time, ctx.steps = start_time, steps
+        ctx.bed_shape = None if bed is None else bed.shape
         ctx.save_for_backward(U0, level_vec, n)
         return U
 
@@ -205,19 +233,24 @@ class _ChunkFunction(torch.autograd.Function):
     def backward(ctx, gU):
         U0, level_vec, n = ctx.saved_tensors
         model = ctx.model
+        need_bed = ctx.bed_shape is not None and ctx.needs_input_grad[3]
         states, dts = _recompute_chunk(model, U0.detach(), level_vec.detach(), float(ctx.t_end),
                                        float(ctx.start_time), ctx.max_dt_cap, ctx.steps)
         lam = gU.contiguous()
         lam_level = torch.zeros_like(level_vec)
         lam_n = torch.zeros_like(n) if model.cfg.apply_friction else None
         B, _, ny, nx = U0.shape
-        ws = AdjointStepper(model, B, ny, nx, U0.device, model._level_arg(level_vec, B)[1])
+        ws = AdjointStepper(model, B, ny, nx, U0.device, model._level_arg(level_vec, B)[1],
+                            bed_grad=need_bed)
+        lv = model._level_arg(level_vec.detach(), B)[0]
         for U_s, dt_s in zip(reversed(states), reversed(dts)):
-            lam, l_lev, lam_n = adjoint_step(model, U_s, level_vec, n, dt_s, lam, ws=ws, lam_n=lam_n)
-            lam_level += l_lev.reshape(lam_level.shape)
+            lam_out, lam = lam, torch.zeros_like(lam)
+            part = ws(U_s, lv, dt_s, lam_out, lam, lam_n)
+            lam_level += ws.level_adjoint(part).reshape(lam_level.shape)
         g_level = lam_level if ctx.needs_input_grad[1] else None
         g_n = lam_n if (ctx.needs_input_grad[2] and lam_n is not None) else None
-        return lam, g_level, g_n, None, None, None, None, None, None
+        g_bed = ws.bed_adjoint().reshape(ctx.bed_shape) if need_bed else None
+        return lam, g_level, g_n, g_bed, None, None, None, None, None, None
 
 
 def _recompute_chunk(model, U0, level_vec, duration, start_time, max_dt_cap, steps):
@@ -264,13 +297,13 @@ def _recompute_chunk(model, U0, level_vec, duration, start_time, max_dt_cap, ste
 def forward_checkpointed(model, U0, t_end, start_time=0.0, boundary_level=None, max_dt_cap=None,
                          max_steps=1_000_000):
     """``model.forward`` over ``t_end`` seconds with a constant (explicit or
-    configured) boundary level, differentiable with respect to U0, the level
-    and the roughness field; only U0 is kept for the backward pass."""
-    _check_no_bed_grad(model)
+    configured) boundary level, differentiable with respect to U0, the level,
+    the roughness field and (when the DEM correction requires grad) the bed;
+    only U0 is kept for the backward pass."""
     level = model._prepare_boundary_level(
         model.cfg.constant_level if boundary_level is None else boundary_level, U0)
     level_vec = level.reshape(-1) if level.ndim > 0 else level.reshape(1)
     steps_out = []
-    U = _ChunkFunction.apply(U0, level_vec, model.roughness_length, model, float(t_end),
-                             float(start_time), max_dt_cap, int(max_steps), steps_out)
+    U = _ChunkFunction.apply(U0, level_vec, model.roughness_length, bed_input(model), model,
+                             float(t_end), float(start_time), max_dt_cap, int(max_steps), steps_out)
     return U

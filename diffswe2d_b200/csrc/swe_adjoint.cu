@@ -36,6 +36,7 @@ struct AdjArgs {
     float* cy;           // y-face contributions [B][ny+1][nx][12]
     float* lS;           // adjoint of S, accumulated (+=)
     float* llevel_part;  // per-block partial level adjoints [B][gridDim.x]
+    float* lbed;         // adjoint of the bed [B,ny,nx], accumulated (+=); BEDG only
     int B, bedB, levelB, ny, nx;
     int bc[4];
     float cval;
@@ -94,7 +95,11 @@ __device__ PrimRec padded_prim(const AdjArgs& a, int b, int j, int i) {
     return prim_rec(U0, U1, U2, z, a.kc);
 }
 
-template <bool DIRY>
+// Face records: 4 cells x (U0, U1, U2[, Z]) floats.
+template <bool BEDG>
+__host__ __device__ constexpr int rec_floats() { return BEDG ? 16 : 12; }
+
+template <bool DIRY, bool BEDG>
 __global__ void adj_face_kernel(const AdjArgs a) {
     const int ny = a.ny, nx = a.nx;
     const long long nfaces = DIRY ? (long long)(ny + 1) * nx : (long long)ny * (nx + 1);
@@ -138,45 +143,57 @@ __global__ void adj_face_kernel(const AdjArgs a) {
         const float l_nL = DIRY ? -r2m : -r1m;
         const float l_tan = DIRY ? (r1p - r1m) : (r2p - r2m);
         CellAdj out[4];
-        face_vjp(P, l_mass, l_nL, l_nR, l_tan, DIRY, a.kc, a.wsr != 0, out);
-        float* dst = (DIRY ? a.cy : a.cx) + (size_t)t * 12;
+        face_vjp<BEDG>(P, l_mass, l_nL, l_nR, l_tan, DIRY, a.kc, a.wsr != 0, out);
+        constexpr int C = BEDG ? 4 : 3;
+        float* dst = (DIRY ? a.cy : a.cx) + (size_t)t * rec_floats<BEDG>();
         for (int s = 0; s < 4; ++s) {
-            dst[3 * s] = out[s].U0;
-            dst[3 * s + 1] = out[s].U1;
-            dst[3 * s + 2] = out[s].U2;
+            dst[C * s] = out[s].U0;
+            dst[C * s + 1] = out[s].U1;
+            dst[C * s + 2] = out[s].U2;
+            if (BEDG) dst[C * s + 3] = out[s].Z;
         }
     }
 }
 
-// Sum of the face contributions to padded cell (row j, column col) along x.
-__device__ void lam_x(const AdjArgs& a, int b, int j, int col, float l[3]) {
-    l[0] = l[1] = l[2] = 0.0f;
+// Sum of the face contributions to padded cell (row j, column col) along x
+// (l[3], the bed channel, with BEDG only).
+template <bool BEDG>
+__device__ void lam_x(const AdjArgs& a, int b, int j, int col, float l[4]) {
+    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
+    l[0] = l[1] = l[2] = l[3] = 0.0f;
     for (int f = col - 1; f <= col + 2; ++f) {
         if (f < 0 || f > a.nx) continue;
-        const float* c = a.cx + ((((size_t)b * a.ny + j) * (a.nx + 1) + f) * 12) + 3 * (col - f + 2);
+        const float* c = a.cx + ((((size_t)b * a.ny + j) * (a.nx + 1) + f) * R) + C * (col - f + 2);
         l[0] += c[0];
         l[1] += c[1];
         l[2] += c[2];
+        if (BEDG) l[3] += c[3];
     }
 }
 
-__device__ void lam_y(const AdjArgs& a, int b, int row, int i, float l[3]) {
-    l[0] = l[1] = l[2] = 0.0f;
+template <bool BEDG>
+__device__ void lam_y(const AdjArgs& a, int b, int row, int i, float l[4]) {
+    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
+    l[0] = l[1] = l[2] = l[3] = 0.0f;
     for (int f = row - 1; f <= row + 2; ++f) {
         if (f < 0 || f > a.ny) continue;
-        const float* c = a.cy + ((((size_t)b * (a.ny + 1) + f) * a.nx + i) * 12) + 3 * (row - f + 2);
+        const float* c = a.cy + ((((size_t)b * (a.ny + 1) + f) * a.nx + i) * R) + C * (row - f + 2);
         l[0] += c[0];
         l[1] += c[1];
         l[2] += c[2];
+        if (BEDG) l[3] += c[3];
     }
 }
 
 // Folds the adjoint lg of ghost g (side `side`; g its column for left/right,
 // row for top/bottom) into cell (j, i) if the ghost was made from it, and
 // adds the level adjoint once per ghost (in the thread of the ghost's
-// clamped source cell).
-__device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float lg[3], int j,
-                           int i, float lam[3], float& llev) {
+// clamped source cell).  BEDG: lg[3] is the ghost's bed adjoint, folded into
+// the cell its bed was copied from (replicate, or periodic), plus the bed
+// terms of the forced ghost depth max(level - z, 0) -> lzc.
+template <bool BEDG>
+__device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float lg[4], int j,
+                           int i, float lam[3], float& llev, float& lzc) {
     const int ny = a.ny, nx = a.nx;
     const bool xs = side < 2;
     const int n = xs ? nx : ny;
@@ -186,6 +203,7 @@ __device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float
     const int periodic = g < 0 ? n + g : g - n;
     const int normal = xs ? 1 : 2;  // momentum channel reflected by a wall
     const int code = a.bc[side];
+    if (BEDG && pos == (code == SWE_BC_PERIODIC ? periodic : clamp_src)) lzc += lg[3];
     switch (code) {
     case SWE_BC_TRANSMISSIVE:
         if (pos == clamp_src) {
@@ -209,7 +227,10 @@ __device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float
             lam[2] += lg[2];
             const float z = bed_of(a, b, xs ? j : clamp_src, xs ? clamp_src : i);
             const float lev = a.level[a.levelB == 1 ? 0 : b];
-            if (lev - z >= 0.0f) llev += lg[0];  // clamp(level - z, min=0)
+            if (lev - z >= 0.0f) {  // clamp(level - z, min=0)
+                llev += lg[0];
+                if (BEDG) lzc -= lg[0];
+            }
         }
         break;
     case SWE_BC_WALL:
@@ -248,7 +269,10 @@ __device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float
             float l_hg = l_diff + (use_hr ? 0.0f : l_hc);
             float l_hr = -l_diff + (use_hr ? l_hc : 0.0f);
             lam[0] += l_hg;
-            if (lev - z >= 0.0f) llev += l_hr;
+            if (lev - z >= 0.0f) {
+                llev += l_hr;
+                if (BEDG) lzc -= l_hr;
+            }
         }
         break;
     default:
@@ -256,6 +280,7 @@ __device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float
     }
 }
 
+template <bool BEDG>
 __global__ void adj_gather_kernel(const AdjArgs a) {
     const int ny = a.ny, nx = a.nx;
     const int b = blockIdx.y;
@@ -265,30 +290,32 @@ __global__ void adj_gather_kernel(const AdjArgs a) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
          t += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(t / nx), i = (int)(t - (long long)(t / nx) * nx);
-        float lam[3], l[3];
-        lam_x(a, b, j, i, lam);
-        lam_y(a, b, j, i, l);
+        float lam[4], l[4];
+        lam_x<BEDG>(a, b, j, i, lam);
+        lam_y<BEDG>(a, b, j, i, l);
         lam[0] += l[0];
         lam[1] += l[1];
         lam[2] += l[2];
+        float lz = BEDG ? lam[3] + l[3] : 0.0f;
         if (i < 2 || i >= nx - 2) {
             const int gx[4] = {-1, -2, nx, nx + 1};
             for (int q = 0; q < 4; ++q) {
-                lam_x(a, b, j, gx[q], l);
-                fold_ghost(a, b, q < 2 ? 0 : 1, gx[q], l, j, i, lam, llev);
+                lam_x<BEDG>(a, b, j, gx[q], l);
+                fold_ghost<BEDG>(a, b, q < 2 ? 0 : 1, gx[q], l, j, i, lam, llev, lz);
             }
         }
         if (j < 2 || j >= ny - 2) {
             const int gy[4] = {-1, -2, ny, ny + 1};
             for (int q = 0; q < 4; ++q) {
-                lam_y(a, b, gy[q], i, l);
-                fold_ghost(a, b, q < 2 ? 2 : 3, gy[q], l, j, i, lam, llev);
+                lam_y<BEDG>(a, b, gy[q], i, l);
+                fold_ghost<BEDG>(a, b, q < 2 ? 2 : 3, gy[q], l, j, i, lam, llev, lz);
             }
         }
         const size_t o = a3(b, 0, j, i, ny, nx);
         a.lS[o] += lam[0];
         a.lS[o + plane] += lam[1];
         a.lS[o + 2 * plane] += lam[2];
+        if (BEDG) a.lbed[(size_t)b * plane + (size_t)j * nx + i] += lz;
     }
     // per-block partial sum of the level adjoint (fixed order)
     __shared__ float s_part[ADJ_THREADS / 32];
@@ -510,11 +537,11 @@ int blocks_for(long long n) {
 
 using namespace swe;
 
-extern "C" int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, int B, int ny, int nx,
-                                   const swe_params* p, const float* level, int levelB,
-                                   const float* lam_rhs, float* scratch_cx, float* scratch_cy,
-                                   float* lam_S, float* level_part, int level_blocks,
-                                   void* stream) {
+namespace {
+int adj_spatial(const float* S, const float* bed, int bedB, int B, int ny, int nx,
+                const swe_params* p, const float* level, int levelB, const float* lam_rhs,
+                float* scratch_cx, float* scratch_cy, float* lam_S, float* level_part,
+                int level_blocks, float* lam_bed, void* stream) {
     if (!S || !bed || !level || !lam_rhs || !scratch_cx || !scratch_cy || !lam_S || !level_part)
         return SWE_EARG;
     if (!valid_params(p) || B < 1 || ny < 2 || nx < 2 || level_blocks < 1) return SWE_EARG;
@@ -528,6 +555,7 @@ extern "C" int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, i
     a.cy = scratch_cy;
     a.lS = lam_S;
     a.llevel_part = level_part;
+    a.lbed = lam_bed;
     a.B = B;
     a.bedB = bedB;
     a.levelB = levelB;
@@ -541,10 +569,37 @@ extern "C" int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, i
     a.wsr = p->water_slope_reset;
     a.kc = make_consts(*p);
     cudaStream_t s = (cudaStream_t)stream;
-    adj_face_kernel<false><<<blocks_for((long long)B * ny * (nx + 1)), ADJ_THREADS, 0, s>>>(a);
-    adj_face_kernel<true><<<blocks_for((long long)B * (ny + 1) * nx), ADJ_THREADS, 0, s>>>(a);
-    adj_gather_kernel<<<dim3(level_blocks, B), ADJ_THREADS, 0, s>>>(a);
+    const int gx = blocks_for((long long)B * ny * (nx + 1)), gy = blocks_for((long long)B * (ny + 1) * nx);
+    if (lam_bed) {
+        adj_face_kernel<false, true><<<gx, ADJ_THREADS, 0, s>>>(a);
+        adj_face_kernel<true, true><<<gy, ADJ_THREADS, 0, s>>>(a);
+        adj_gather_kernel<true><<<dim3(level_blocks, B), ADJ_THREADS, 0, s>>>(a);
+    } else {
+        adj_face_kernel<false, false><<<gx, ADJ_THREADS, 0, s>>>(a);
+        adj_face_kernel<true, false><<<gy, ADJ_THREADS, 0, s>>>(a);
+        adj_gather_kernel<false><<<dim3(level_blocks, B), ADJ_THREADS, 0, s>>>(a);
+    }
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+}
+}  // namespace
+
+extern "C" int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, int B, int ny, int nx,
+                                   const swe_params* p, const float* level, int levelB,
+                                   const float* lam_rhs, float* scratch_cx, float* scratch_cy,
+                                   float* lam_S, float* level_part, int level_blocks,
+                                   void* stream) {
+    return adj_spatial(S, bed, bedB, B, ny, nx, p, level, levelB, lam_rhs, scratch_cx, scratch_cy,
+                       lam_S, level_part, level_blocks, nullptr, stream);
+}
+
+extern "C" int swe_adj_spatial_bed_f32(const float* S, const float* bed, int bedB, int B, int ny,
+                                       int nx, const swe_params* p, const float* level, int levelB,
+                                       const float* lam_rhs, float* scratch_cx, float* scratch_cy,
+                                       float* lam_S, float* level_part, int level_blocks,
+                                       float* lam_bed, void* stream) {
+    if (!lam_bed) return SWE_EARG;
+    return adj_spatial(S, bed, bedB, B, ny, nx, p, level, levelB, lam_rhs, scratch_cx, scratch_cy,
+                       lam_S, level_part, level_blocks, lam_bed, stream);
 }
 
 namespace {

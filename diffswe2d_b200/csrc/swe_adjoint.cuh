@@ -10,7 +10,9 @@
 //   abs, sign                sign(x) and 0 (both 0 at x = 0)
 //   sqrt                     grad / (2 sqrt(x)); x / y: grad / y and
 //                            -grad (x / y) / y
-// The bed is not differentiated (bed inversion is outside this path).
+// The bed is differentiated on request (template flag BEDG: the gradient
+// of the DEM-correction inversion, src/solver.py:111-147); without it the
+// bed's adjoint is not formed.
 #pragma once
 
 #include "swe_math.cuh"
@@ -98,8 +100,9 @@ SWE_HD PrimRec prim_rec(float U0, float U1, float U2, float z, const SweConsts& 
 // reconstruction.py:23-24, :71-73): lh includes everything that reached h
 // (directly, via eta and via the reconstruction's own clamp of h).
 SWE_HD void prim_bwd(const PrimRec& p, float lh, float lsafe, float lu, float lv, float leta,
-                     const SweConsts& k, float& lU0, float& lU1, float& lU2) {
+                     const SweConsts& k, float& lU0, float& lU1, float& lU2, float& lz) {
     lh += leta;
+    lz += leta;  // eta = h + bed
     if (p.wet) {
         lU1 += quot(lu, p.safe, p.rsafe);
         lU2 += quot(lv, p.safe, p.rsafe);
@@ -164,12 +167,13 @@ SWE_HD SideRec side_fwd(const PrimRec& a, const PrimRec& c, const PrimRec& b, bo
 
 // Adjoints of the three cells' primitives (h, safe, u, v, eta per cell).
 struct PrimAdj {
-    float h, safe, u, v, eta;
+    float h, safe, u, v, eta, z;
 };
 
+template <bool BEDG>
 SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin, float l_eta,
-                     float l_u, float l_v, const SweConsts& k, PrimAdj& la, PrimAdj& lc,
-                     PrimAdj& lb) {
+                     float l_u, float l_v, float l_bed, const SweConsts& k, PrimAdj& la,
+                     PrimAdj& lc, PrimAdj& lb) {
     const float sg = plus ? 1.0f : -1.0f;
     // u_side = u +/- (0.5 f) du ; v likewise
     const float hf = 0.5f * r.f;
@@ -190,10 +194,17 @@ SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin
     l_dh += sg * (0.5f * l_hlin);
     lc.eta += l_eta;
     float l_deta = sg * (0.5f * l_eta);
-    if (r.reset) {  // deta = dh + dz (dz carries no gradient)
+    float l_dz = 0.0f;
+    if (BEDG) {  // bed_side = bed +/- 0.5 dz
+        lc.z += l_bed;
+        l_dz = sg * (0.5f * l_bed);
+    }
+    if (r.reset) {  // deta = dh + dz
         l_dh += l_deta;
+        if (BEDG) l_dz += l_deta;
         l_deta = 0.0f;
     }
+    if (BEDG) incr_bwd(r.iz, l_dz, k.theta, la.z, lc.z, lb.z);
     incr_bwd(r.ih, l_dh, k.theta, la.h, lc.h, lb.h);
     incr_bwd(r.ie, l_deta, k.theta, la.eta, lc.eta, lb.eta);
     incr_bwd(r.iu, l_du, k.theta, la.u, lc.u, lb.u);
@@ -205,9 +216,10 @@ SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin
 // (mass flux, normal flux minus source_L, normal flux minus source_R,
 // tangential flux).  Outputs: adjoints of (U0, U1, U2) of the four cells.
 struct CellAdj {
-    float U0, U1, U2;
+    float U0, U1, U2, Z;  // Z: adjoint of the cell's bed (BEDG only)
 };
 
+template <bool BEDG>
 SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, float l_tan,
                      bool normal_y, const SweConsts& k, bool wsr, CellAdj out[4]) {
     // ---- forward: sides of p1 ("p") and p2 ("m")
@@ -398,6 +410,10 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
         l_bcn -= l_srcR * sR1;
         la[2].h += k.half_g * l_s2;
         l_hcR += k.half_g * l_s2;
+        if (BEDG) {  // srcL = (g/2 (h1 + hcL)) (z1 - bcn), srcR likewise with z2
+            la[1].z += l_srcL * sL1;
+            la[2].z += l_srcR * sR1;
+        }
     }
     // hc = clamp(min(eta_side - bcn, hlin), min=0)
     const float l_mL = mL >= 0.0f ? l_hcL : 0.0f;
@@ -409,19 +425,27 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     const float l_AR = l_mR * sa, l_Rhlin = l_mR * sb;
     float l_Leta = l_AL, l_Reta = l_AR;
     l_bcn -= l_AL + l_AR;
-    // bcn = min(baud, min(etaL, etaR)); baud (bed only) carries no gradient
+    // bcn = min(baud, min(etaL, etaR)); baud = max(bedL, bedR)
     minmax_shares(baud, inner, false, sa, sb);
     const float l_inner = l_bcn * sb;
+    float l_Lbed = 0.0f, l_Rbed = 0.0f;
+    if (BEDG) {
+        const float l_baud = l_bcn * sa;
+        float ba, bb;
+        minmax_shares(Lp.bed, Rm.bed, true, ba, bb);
+        l_Lbed = l_baud * ba;
+        l_Rbed = l_baud * bb;
+    }
     minmax_shares(Lp.eta, Rm.eta, false, sa, sb);
     l_Leta += l_inner * sa;
     l_Reta += l_inner * sb;
     // sides -> primitives of the four cells
-    side_bwd(SL_, P[1], true, l_Lhlin, l_Leta, l_Lu, l_Lv, k, la[0], la[1], la[2]);
-    side_bwd(SR_, P[2], false, l_Rhlin, l_Reta, l_Ru, l_Rv, k, la[1], la[2], la[3]);
+    side_bwd<BEDG>(SL_, P[1], true, l_Lhlin, l_Leta, l_Lu, l_Lv, l_Lbed, k, la[0], la[1], la[2]);
+    side_bwd<BEDG>(SR_, P[2], false, l_Rhlin, l_Reta, l_Ru, l_Rv, l_Rbed, k, la[1], la[2], la[3]);
     for (int i = 0; i < 4; ++i) {
-        out[i].U0 = out[i].U1 = out[i].U2 = 0.0f;
+        out[i].U0 = out[i].U1 = out[i].U2 = out[i].Z = 0.0f;
         prim_bwd(P[i], la[i].h, la[i].safe, la[i].u, la[i].v, la[i].eta, k, out[i].U0, out[i].U1,
-                 out[i].U2);
+                 out[i].U2, out[i].Z);
     }
 }
 

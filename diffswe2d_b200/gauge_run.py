@@ -31,7 +31,7 @@ from typing import Optional, Sequence, Tuple
 import torch
 
 from . import _native as nat
-from .adjoint import LEVEL_BLOCKS, AdjointStepper, _check_no_bed_grad
+from .adjoint import LEVEL_BLOCKS, AdjointStepper, bed_input
 
 GRAPH_STEPS = 32
 CHECKPOINT_EVERY = 128
@@ -63,6 +63,7 @@ class GaugeRunWorkspace:
         self.levels = torch.zeros((n_out, levelB), device=dev)
         self.lv = torch.zeros(levelB, device=dev)
         self.ngauge = len(gauges)
+        self.gauge_cells = [(int(iy), int(ix)) for iy, ix in gauges]
         for iy, ix in gauges:
             if not (0 <= iy < ny and 0 <= ix < nx):
                 raise ValueError(f"gauge cell {(iy, ix)} outside the {ny}x{nx} grid")
@@ -185,9 +186,10 @@ class GaugeRunWorkspace:
             self.replay_graph = g
         self.replay_graph.replay()
 
-    def _alloc_backward(self):
+    def _alloc_backward(self, bed_grad: bool):
         dev, shape = self.dev, self.bufs[0].shape
-        self.stepper = AdjointStepper(self.model, self.B, self.ny, self.nx, dev, self.levelB)
+        self.stepper = AdjointStepper(self.model, self.B, self.ny, self.nx, dev, self.levelB,
+                                      bed_grad=bed_grad)
         self.lam = [torch.empty(shape, device=dev), torch.empty(shape, device=dev)]
         self.g_gauge = torch.zeros_like(self.gauge_out)
         self.g_levels = torch.zeros_like(self.levels)
@@ -217,15 +219,18 @@ class GaugeRunWorkspace:
                 LEVEL_BLOCKS, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)
             nat.check(rc, "gauge-run adjoint finish")
 
-    def backward(self, g_gauges, g_final):
-        """Adjoints of U0, the levels [n_out, levelB] and the roughness field
-        for the cotangents of the gauges [B, n_out, ngauge] and of the final
-        state (either may be None).  The last segment's adjoint steps are
-        enqueued directly; every full segment replays one captured graph of
-        checkpoint_every adjoint steps.  No host synchronisation."""
+    def backward(self, g_gauges, g_final, bed_grad: bool = False):
+        """Adjoints of U0, the levels [n_out, levelB], the roughness field and
+        (bed_grad) the bed for the cotangents of the gauges [B, n_out, ngauge]
+        and of the final state (either may be None).  The last segment's
+        adjoint steps are enqueued directly; every full segment replays one
+        captured graph of checkpoint_every adjoint steps.  No host
+        synchronisation."""
         total = self.last_steps
-        if self.stepper is None:
-            self._alloc_backward()
+        if self.stepper is None or self.stepper.bed_grad != bool(bed_grad):
+            self._alloc_backward(bool(bed_grad))
+        if self.stepper.bed_grad:
+            self.stepper.lam_bed.zero_()
         if g_final is None:
             self.lam[0].zero_()
         else:
@@ -242,7 +247,8 @@ class GaugeRunWorkspace:
         with sweep_rows(self.rows):
             self._backward_segments(nseg, total)
         lam_n = self.lam_n.clone() if self.lam_n is not None else None
-        return self.lam[0].clone(), self.g_levels.clone(), lam_n
+        lam_bed = self.stepper.bed_adjoint().clone() if self.stepper.bed_grad else None
+        return self.lam[0].clone(), self.g_levels.clone(), lam_n, lam_bed
 
     def _backward_segments(self, nseg, total):
         for j in range(nseg - 1, -1, -1):
@@ -272,11 +278,12 @@ class _RecordFull(RuntimeError):
 
 class _GaugeRunFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, U0, levels, n, ws, out_dt, max_dt_cap, max_steps):
+    def forward(ctx, U0, levels, n, bed, ws, out_dt, max_dt_cap, max_steps):
         lv = levels.detach().t() if levels.ndim == 2 else levels.detach().reshape(-1, 1)
         gauges, final = ws.run(U0.detach(), lv, out_dt, max_dt_cap, max_steps)
         ctx.ws, ctx.generation = ws, ws.generation
         ctx.levels_shape = levels.shape
+        ctx.bed_shape = None if bed is None else bed.shape
         return gauges.clone(), final.clone()
 
     @staticmethod
@@ -285,12 +292,23 @@ class _GaugeRunFunction(torch.autograd.Function):
         if ws.generation != ctx.generation:
             raise RuntimeError("the gauge-run workspace ran again before this run's backward pass; "
                                "call backward before the next gauge_run of the same shape")
-        lam, g_levels, lam_n = ws.backward(g_gauges, g_final)
+        need_bed = ctx.bed_shape is not None and ctx.needs_input_grad[3]
+        lam, g_levels, lam_n, lam_bed = ws.backward(g_gauges, g_final, need_bed)
         g_lv = None
         if ctx.needs_input_grad[1]:
             g_lv = (g_levels.t() if len(ctx.levels_shape) == 2 else g_levels).reshape(ctx.levels_shape)
         g_n = lam_n if (ctx.needs_input_grad[2] and lam_n is not None) else None
-        return lam if ctx.needs_input_grad[0] else None, g_lv, g_n, None, None, None, None
+        g_bed = None
+        if need_bed:
+            # eta = h + bed at the gauges: the bed term's adjoint (summed over intervals)
+            if g_gauges is not None and ws.ngauge:
+                per = g_gauges.sum(dim=1)  # [B, ngauge]
+                if lam_bed.shape[0] == 1:
+                    per = per.sum(dim=0, keepdim=True)
+                for q, (iy, ix) in enumerate(ws.gauge_cells):
+                    lam_bed[:, 0, iy, ix] += per[:, q]
+            g_bed = lam_bed.reshape(ctx.bed_shape)
+        return lam if ctx.needs_input_grad[0] else None, g_lv, g_n, g_bed, None, None, None, None
 
 
 _WORKSPACES = {}
@@ -306,9 +324,8 @@ def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
 
     Returns ``(gauges, U_final)``: eta = h + bed at the gauge cells (row,
     column) after every interval, [B, n_out, len(gauges)], and the final
-    state.  Differentiable with respect to U0, levels and the roughness
-    field."""
-    _check_no_bed_grad(model)
+    state.  Differentiable with respect to U0, levels, the roughness field
+    and (when the DEM correction requires grad) the bed."""
     model._check_state(U0)
     U0 = nat.require_cuda_f32("U0", U0)
     B, _, ny, nx = U0.shape
@@ -335,8 +352,8 @@ def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
     levels_f = levels.to(dtype=torch.float32)
     while True:
         try:
-            return _GaugeRunFunction.apply(U0, levels_f, model.roughness_length, ws, float(out_dt),
-                                           max_dt_cap, int(max_steps))
+            return _GaugeRunFunction.apply(U0, levels_f, model.roughness_length, bed_input(model), ws,
+                                           float(out_dt), max_dt_cap, int(max_steps))
         except _RecordFull as e:
             ws = GaugeRunWorkspace(model, B, ny, nx, U0.device, levelB, n_out, gauges, graph_steps,
                                    checkpoint_every, record_cap=4 * e.steps)

@@ -84,6 +84,24 @@ class SWE2D(nn.Module):
             correction = float(self.maximum_dem_correction) * torch.tanh(correction)
         return self.bed_reference + correction * self.valid_mask.to(self.bed_reference.dtype)
 
+    def dem_regularization(self, prior_weight=1.0, slope_weight=0.0, curvature_weight=0.0):
+        """Prior, slope and curvature penalty of the DEM-correction inversion
+        (src/solver.py:807-836): mean squared correction, mean squared first
+        differences of the bed along x and y, mean squared second
+        differences; PyTorch operations on the bed (autograd supplies their
+        gradient, the hand-written adjoint the simulation's)."""
+        bed = self.bed
+        correction = bed - self.bed_reference
+        d_x = bed[..., 1:] - bed[..., :-1]
+        d_y = bed[..., 1:, :] - bed[..., :-1, :]
+        prior = correction.square().mean()
+        slope = d_x.square().mean() + d_y.square().mean()
+        zero = bed.new_zeros(())
+        curv_x = (d_x[..., 1:] - d_x[..., :-1]).square().mean() if d_x.shape[-1] >= 2 else zero
+        curv_y = (d_y[..., 1:, :] - d_y[..., :-1, :]).square().mean() if d_y.shape[-2] >= 2 else zero
+        return (float(prior_weight) * prior + float(slope_weight) * slope
+                + float(curvature_weight) * (curv_x + curv_y))
+
     # ------------------------------------------------------ configuration
     def set_dynamic_boundary(self, times: torch.Tensor, water_levels: torch.Tensor,
                              enabled: bool = True) -> None:
@@ -271,11 +289,13 @@ class SWE2D(nn.Module):
 
     def _needs_adjoint(self, U, boundary_level) -> bool:
         """A step is differentiated when autograd is on and the state, the
-        boundary level or the roughness field requires grad."""
+        boundary level, the roughness field or the DEM correction requires
+        grad."""
         if not torch.is_grad_enabled():
             return False
-        return bool(U.requires_grad or self.roughness_length.requires_grad or (
-            torch.is_tensor(boundary_level) and boundary_level.requires_grad))
+        return bool(U.requires_grad or self.roughness_length.requires_grad
+                    or self.dem_correction_parameter.requires_grad
+                    or (torch.is_tensor(boundary_level) and boundary_level.requires_grad))
 
     def _launch_step(self, U, level, max_dt_f, infiltration, red=None, scratch=None):
         """Enqueue one step; returns (U_new, status, dt) with one host read."""

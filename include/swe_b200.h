@@ -267,6 +267,22 @@ int swe_adj_spatial_f32(const float* S, const float* bed, int bedB, int B, int n
                         float* level_part, int level_blocks, void* stream);
 
 /*
+ * swe_adj_spatial_f32 plus the adjoint of the bed (the DEM-correction
+ * inversion's gradient, src/solver.py:111-147 under autograd):
+ * lam_bed[b,j,i] += d(rhs)/d(bed[b or 0, j, i])^T lam_rhs, per batch member
+ * ([B,ny,nx]; the caller sums over b when bedB = 1).  The bed enters through
+ * eta = h + z, its limited increments and face values, the Audusse bed,
+ * the well-balanced sources and the ghost cells (replicated or periodic
+ * copies, forced depth max(level - z, 0)).  Scratch as above but 16 floats
+ * per face (B*ny*(nx+1)*16 and B*(ny+1)*nx*16).
+ */
+int swe_adj_spatial_bed_f32(const float* S, const float* bed, int bedB, int B, int ny, int nx,
+                            const swe_params* p, const float* level, int levelB,
+                            const float* lam_rhs, float* scratch_cx, float* scratch_cy,
+                            float* lam_S, float* level_part, int level_blocks, float* lam_bed,
+                            void* stream);
+
+/*
  * Pointwise parts of the step adjoint, for step input U, tendency k and
  * time step dt:
  *   mode 0: corrector and friction (solver.py:646-661, friction.py:12-131):

@@ -18,6 +18,13 @@ adj_run_wet.npz  the same on a crop across the shoreline (92 % wet at the
               start), where U0 and n have smooth gradients for finite
               differences (every U0 entry of the dry crop sits on the wet/dry
               kink).
+adj_bed.npz   gradients w.r.t. dem_correction_parameter (the bed of the
+              DEM-correction inversion, src/solver.py:111-147): the one-step
+              cases of adj_step.npz with train_dem=True, one case with the
+              tanh bound (maximum_dem_correction=0.05), a partial valid mask
+              and a nonzero correction; and the 30-step loss of
+              adj_run_wet.npz plus dem_regularization(1.0, 0.1, 0.01)
+              (src/solver.py:807-836) with the same bound.
 """
 from __future__ import annotations
 
@@ -65,6 +72,64 @@ def _grads_step(ref, dtype, cfg_kw, U, bed, n, level, w, dx, dy, max_dt):
     gn = (m.roughness_length.grad.numpy().astype(np.float64) if m.roughness_length.grad is not None
           else np.zeros((1, 1) + n.shape, np.float64))
     return Ut.grad.numpy().astype(np.float64), gl, gn, dt
+
+
+def _grads_step_bed(ref, dtype, cfg_kw, U, bed, n, level, w, dx, dy, max_dt, max_corr=None,
+                    mask=None, corr0=None):
+    cfg = ref.SWEConfig(**cfg_kw, constant_value=0.05)
+    m = ref.SWE2D(torch.from_numpy(bed).to(dtype), torch.from_numpy(n).to(dtype), dx, dy, config=cfg,
+                  train_dem=True, maximum_dem_correction=max_corr,
+                  valid_mask=None if mask is None else torch.from_numpy(mask))
+    if corr0 is not None:
+        with torch.no_grad():
+            m.dem_correction_parameter.copy_(torch.from_numpy(corr0).to(dtype).reshape(
+                m.dem_correction_parameter.shape))
+    Un, _ = m.step(torch.from_numpy(U).to(dtype), 0.0, max_dt, boundary_level=level)
+    (Un * torch.from_numpy(w).to(dtype)).sum().backward()
+    return m.dem_correction_parameter.grad.numpy().astype(np.float64)
+
+
+def make_bed_grads(ref, out):
+    d = dict(np.load(out / "adj_step.npz"))
+    rng = np.random.default_rng(78)
+    mask = rng.uniform(size=d["bed"].shape) > 0.2
+    corr0 = (rng.normal(size=d["bed"].shape) * 0.5).astype(np.float32)
+    g = {"mask": mask, "corr0": corr0}
+    for name, kw in STEP_CASES.items():
+        field = d["z0"] if kw.get("frictionmodel") == "roughness_length" else d["n"]
+        args = (kw, d["U"], d["bed"], field, 0.18, d["w"], 0.05, 0.04, 0.01)
+        with correctly_rounded_elementary():
+            g[f"{name}_gbed"] = _grads_step_bed(ref, torch.float32, *args)
+        g[f"{name}_gbed64"] = _grads_step_bed(ref, torch.float64, *args)
+    kw = STEP_CASES["water_level"]
+    args = (kw, d["U"], d["bed"], d["n"], 0.18, d["w"], 0.05, 0.04, 0.01)
+    with correctly_rounded_elementary():
+        g["tanh_mask_gbed"] = _grads_step_bed(ref, torch.float32, *args, 0.05, mask, corr0)
+    g["tanh_mask_gbed64"] = _grads_step_bed(ref, torch.float64, *args, 0.05, mask, corr0)
+    # 30-step run on the shoreline crop with the DEM regulariser
+    r = dict(np.load(out / "adj_run_wet.npz"))
+    corr_run = (rng.normal(size=r["bed"].shape) * 0.3).astype(np.float32)
+    g["run_corr0"] = corr_run
+    kw = dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+              boundary_bottom="wall")
+    for dtype, tag, cr in ((torch.float32, "f32", True), (torch.float64, "f64", False)):
+        m = ref.SWE2D(torch.from_numpy(r["bed"]).to(dtype), torch.from_numpy(r["n"]).to(dtype),
+                      float(r["dx"]), float(r["dx"]), config=ref.SWEConfig(**kw), train_dem=True,
+                      maximum_dem_correction=0.05)
+        with torch.no_grad():
+            m.dem_correction_parameter.copy_(torch.from_numpy(corr_run).to(dtype).reshape(
+                m.dem_correction_parameter.shape))
+        ctx = correctly_rounded_elementary() if cr else _Null()
+        with ctx:
+            loss = run_loss(m, dtype, torch.from_numpy(r["U0"]).to(dtype),
+                            torch.from_numpy(r["levels"]).to(dtype), RUN_GAUGES, m.bed[0, 0], None,
+                            None, float(r["dx"]))
+            loss = loss + m.dem_regularization(1.0, 0.1, 0.01)
+            loss.backward()
+        g[f"run_{tag}_loss"] = float(loss)
+        g[f"run_{tag}_gcorr"] = m.dem_correction_parameter.grad.numpy().astype(np.float64)
+    np.savez_compressed(out / "adj_bed.npz", **g)
+    print("adj_bed.npz", g["run_f32_loss"], g["run_f64_loss"])
 
 
 def make_step_grads(ref, out):
@@ -149,3 +214,4 @@ def make_adjoint(ref, out):
     make_step_grads(ref, out)
     make_run_grads(ref, out)
     make_run_grads(ref, out, "adj_run_wet", 100, 170)
+    make_bed_grads(ref, out)

@@ -231,3 +231,99 @@ def test_checkpointed_chunk_matches_stepwise_autograd(golden):
     assert _rel(g0c, g0s) <= 1e-6
     assert abs(glc - gls) <= 1e-6 * max(abs(gls), 1e-30)
     assert _rel(gnc, gns) <= 1e-6
+
+
+# ---------------------------------------------------------------- bed (DEM)
+def _bed_model(cfg_kw, bed, field, dx, dy, max_corr=None, mask=None, corr0=None):
+    cfg = SWEConfig(**cfg_kw, constant_value=0.05)
+    m = SWE2D(_t(bed), _t(field), dx, dy, config=cfg, train_dem=True, maximum_dem_correction=max_corr,
+              valid_mask=None if mask is None else torch.from_numpy(mask).to(DEV))
+    if corr0 is not None:
+        with torch.no_grad():
+            m.dem_correction_parameter.copy_(_t(corr0).reshape(m.dem_correction_parameter.shape))
+    return m
+
+
+@pytest.mark.parametrize("case", sorted(STEP_CASES) + ["tanh_mask"])
+def test_one_step_bed_gradient_matches_reference_autograd(golden, case):
+    """d(sum w U_new)/d(dem_correction_parameter): the bed's adjoint through
+    the spatial operator (eta, increments, Audusse bed, sources, ghost cells)
+    chained by autograd through the tanh bound and mask."""
+    d, g = golden("adj_step"), golden("adj_bed")
+    if case == "tanh_mask":
+        m = _bed_model(STEP_CASES["water_level"], d["bed"], d["n"], 0.05, 0.04, 0.05, g["mask"], g["corr0"])
+    else:
+        kw = STEP_CASES[case]
+        field = d["z0"] if kw.get("frictionmodel") == "roughness_length" else d["n"]
+        m = _bed_model(kw, d["bed"], field, 0.05, 0.04)
+    Un, _ = m.step(_t(d["U"]), 0.0, 0.01, boundary_level=torch.tensor(0.18, device=DEV))
+    (Un * _t(d["w"])).sum().backward()
+    gb = m.dem_correction_parameter.grad.cpu().numpy()
+    e = _rel(gb, g[f"{case}_gbed"])
+    print(case, "d/dbed", e, "vs FP64", _rel(gb, g[f"{case}_gbed64"]))
+    assert e <= TOL
+
+
+def test_thirty_step_bed_gradient_with_regulariser_matches_reference(golden):
+    """30 steps on the shoreline crop, gauge loss + dem_regularization(1, 0.1,
+    0.01), bounded correction: the gradient w.r.t. dem_correction_parameter,
+    stepwise autograd nodes and one forward_checkpointed node."""
+    r, g = golden("adj_run_wet"), golden("adj_bed")
+    cfg_kw = dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                  boundary_bottom="wall")
+    for mode in ("steps", "chunk"):
+        m = SWE2D(_t(r["bed"]), _t(r["n"]), float(r["dx"]), float(r["dx"]), config=SWEConfig(**cfg_kw),
+                  train_dem=True, maximum_dem_correction=0.05)
+        with torch.no_grad():
+            m.dem_correction_parameter.copy_(_t(g["run_corr0"]).reshape(m.dem_correction_parameter.shape))
+        if mode == "steps":
+            loss = _run_loss(m, _t(r["U0"]), _t(r["levels"]), r["gauges"], m.bed[0, 0])
+        else:  # one node per step (constant levels differ per step, so chunk = 1 step each)
+            U, loss = _t(r["U0"]), 0.0
+            for s in range(r["levels"].shape[0]):
+                U = forward_checkpointed(m, U, t_end=2.0e-3, boundary_level=_t(r["levels"])[s])
+                for iy, ix in r["gauges"]:
+                    loss = loss + (U[0, 0, iy, ix] + m.bed[0, 0, iy, ix]) ** 2
+            loss = loss + 1e-3 * (U * U).sum()
+        loss = loss + m.dem_regularization(1.0, 0.1, 0.01)
+        loss.backward()
+        assert float(loss.detach()) == pytest.approx(float(g["run_f32_loss"]), rel=2e-6)
+        gc = m.dem_correction_parameter.grad.cpu().numpy()
+        e = _rel(gc, g["run_f32_gcorr"])
+        print(mode, "d/dcorrection", e, "vs FP64", _rel(gc, g["run_f64_gcorr"]))
+        assert e <= TOL
+
+
+def test_bed_gradient_matches_fp64_finite_differences(golden):
+    """Central differences (eps 1e-7 m) of the 30-step gauge loss w.r.t. bed
+    entries of wet cells, FP64 oracle.  The loss is piecewise smooth in the
+    bed as in the depth (eta = h + z feeds the limiters), so the bar is the
+    depth entries' 2 %."""
+    d = golden("adj_run_wet")
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall")
+    m = SWE2D(_t(d["bed"]), _t(d["n"]), float(d["dx"]), float(d["dx"]), config=cfg, train_dem=True)
+    _run_loss(m, _t(d["U0"]), _t(d["levels"]), d["gauges"], m.bed[0, 0]).backward()
+    gb = m.dem_correction_parameter.grad.cpu().numpy().reshape(d["bed"].shape)
+
+    def loss64(bed):
+        om = OracleSWE(bed, d["n"].astype(np.float64), float(d["dx"]), float(d["dx"]), cfg,
+                       dtype=np.float64)
+        U = d["U0"].astype(np.float64)
+        L = 0.0
+        for s in range(len(d["levels"])):
+            U, _ = om.step(U, 0.0, 2.0e-3, boundary_level=float(d["levels"][s]))
+            for iy, ix in d["gauges"]:
+                L += (U[0, 0, iy, ix] + float(bed[iy, ix])) ** 2
+        return L + 1e-3 * float((U * U).sum())
+
+    bed64 = d["bed"].astype(np.float64)
+    wet = (d["U0"][0, 0] > 5e-3).ravel()
+    order = [i for i in np.argsort(-np.abs(gb).ravel()) if wet[i]][:4]
+    for idx in order:
+        up, dn = bed64.ravel().copy(), bed64.ravel().copy()
+        up[idx] += 1e-7
+        dn[idx] -= 1e-7
+        fd = (loss64(up.reshape(bed64.shape)) - loss64(dn.reshape(bed64.shape))) / 2e-7
+        print("bed", idx, gb.ravel()[idx], fd)
+        assert abs(gb.ravel()[idx] - fd) <= 2e-2 * abs(fd)
