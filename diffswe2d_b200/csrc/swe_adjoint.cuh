@@ -443,7 +443,8 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     side_bwd<BEDG>(SL_, P[1], true, l_Lhlin, l_Leta, l_Lu, l_Lv, l_Lbed, k, la[0], la[1], la[2]);
     side_bwd<BEDG>(SR_, P[2], false, l_Rhlin, l_Reta, l_Ru, l_Rv, l_Rbed, k, la[1], la[2], la[3]);
     for (int i = 0; i < 4; ++i) {
-        out[i].U0 = out[i].U1 = out[i].U2 = out[i].Z = 0.0f;
+        out[i].U0 = out[i].U1 = out[i].U2 = 0.0f;
+        out[i].Z = la[i].z;  // sources, increments, face beds; prim_bwd adds the eta term
         prim_bwd(P[i], la[i].h, la[i].safe, la[i].u, la[i].v, la[i].eta, k, out[i].U0, out[i].U1,
                  out[i].U2, out[i].Z);
     }
