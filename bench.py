@@ -397,6 +397,10 @@ def run_warmstart(args, world, rank, local):
                    "held_out_cases": args.ws_cases, "tol_m": 1e-4, "lr": 0.002,
                    "max_iters": args.ws_max_iters, "samples": 1125, "gauges": 6, "controls": 16},
         "warm": {"reached": res["warm"]["reached"], "median_iterations": res["warm"]["median_iterations"],
+                 "max_iterations": max([i for i in res["warm"]["iterations"] if i is not None], default=None),
+                 "mean_iterations": (float(np.mean([i for i in res["warm"]["iterations"] if i is not None]))
+                                     if res["warm"]["reached"] else None),
+                 "max_seconds_to_tol": max(warm_t) if warm_t else None,
                  "median_seconds_to_tol": float(np.median(warm_t)) if warm_t else None,
                  "seconds_per_iteration": res["warm"]["seconds_per_iteration"],
                  "median_initial_rmse": float(np.median(res["warm"]["initial_rmse"])),

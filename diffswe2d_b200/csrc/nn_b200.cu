@@ -130,12 +130,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 // 2-D tiled TMA load of box (x = column, y = row) into shared memory,
 // completion counted on mbarrier `bar`.  x is a multiple of 8 bf16
 // elements (16 bytes), as the tensor map's inner box.
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            uint32_t bar) {
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, uint64_t map, int x, int y, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
         "[%0], [%1, {%2, %3}], [%4];"
-        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar)
         : "memory");
 }
 
@@ -170,6 +169,31 @@ __device__ __forceinline__ void epilogue_store(const GemmArgs& g, int r, int c, 
     if (g.out_bf16) g.out_bf16[o] = __bfloat16_as_ushort(__float2bfloat16_rn(y));
 }
 
+// 16-wide K steps of the K block starting at k0 that lie before kend (K and
+// the split ends are multiples of 16).
+__device__ __forceinline__ int k_steps(int k0, int kend) {
+    const int rem = kend - k0;
+    return rem >= BK ? BK / 16 : rem / 16;
+}
+
+// Thread 0 arms stage kb's "full" barrier with the bytes of the slabs it is
+// about to copy and issues one TMA copy per 8-column slab of A and B that
+// lies before kend (slabs past the end of K are not copied and not read).
+__device__ void tma_stage(uint8_t* smem, uint64_t* s_full, int kb, int kbeg, int kend, int m0, int n0,
+                          int bn, uint64_t mapA, uint64_t mapB) {
+    const int s = kb & 1;
+    uint8_t* sA = smem + s * STAGE_BYTES;
+    uint8_t* sB = sA + A_BYTES;
+    const uint32_t bar = smem_u32(&s_full[s]);
+    const int k0 = kbeg + kb * BK;
+    const int nslab = 2 * k_steps(k0, kend);
+    mbar_expect_tx(bar, (uint32_t)nslab * (uint32_t)(BM + bn) * 16u);
+    for (int kc = 0; kc < nslab; ++kc) {
+        tma_load_2d(smem_u32(sA + kc * (BM * 16)), mapA, k0 + kc * 8, m0, bar);
+        tma_load_2d(smem_u32(sB + kc * (bn * 16)), mapB, k0 + kc * 8, n0, bar);
+    }
+}
+
 template <bool TMA>
 __global__ void __launch_bounds__(NT, 1)
 gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
@@ -187,7 +211,6 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
     const int kbeg = blockIdx.z * g.kchunk;
     const int kend = min(g.K, kbeg + g.kchunk);
     const int nkb = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
-    const uint32_t stage_tx = (uint32_t)(BM + bn) * BK * 2;  // bytes landed per stage
     uint32_t ncols = 32;
     while ((int)ncols < bn) ncols <<= 1;
 
@@ -212,23 +235,11 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
     uint32_t ph_full[2] = {0u, 0u}, ph_empty[2] = {0u, 0u};
     int issued = 0;     // MMA groups committed
     int loaded = 0;     // TMA stages armed (TMA path)
+    uint32_t err_code = 0u;  // which bounded wait gave up (thread 0)
 
-    // TMA path: thread 0 arms stage kb's "full" barrier and copies its slabs.
-    auto tma_stage = [&](int kb) {
-        const int s = kb & 1;
-        uint8_t* sA = smem + s * STAGE_BYTES;
-        uint8_t* sB = sA + A_BYTES;
-        const uint32_t bar = smem_u32(&s_full[s]);
-        mbar_expect_tx(bar, stage_tx);
-        const int k0 = kbeg + kb * BK;
-#pragma unroll
-        for (int kc = 0; kc < BK / 8; ++kc) {
-            tma_load_2d(smem_u32(sA + kc * (BM * 16)), &tmA, k0 + kc * 8, m0, bar);
-            tma_load_2d(smem_u32(sB + kc * (bn * 16)), &tmB, k0 + kc * 8, n0, bar);
-        }
-    };
+    const uint64_t mapA = reinterpret_cast<uint64_t>(&tmA), mapB = reinterpret_cast<uint64_t>(&tmB);
     if (TMA && tid == 0 && nkb > 0) {
-        tma_stage(0);
+        tma_stage(smem, s_full, 0, kbeg, kend, m0, n0, bn, mapA, mapB);
         loaded = 1;
     }
 
@@ -246,19 +257,22 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
                         if (ok) ph_empty[s1] ^= 1u;
                     }
                     if (ok) {
-                        tma_stage(kb + 1);
+                        tma_stage(smem, s_full, kb + 1, kbeg, kend, m0, n0, bn, mapA, mapB);
                         loaded = kb + 2;
+                    } else {
+                        err_code = 0x10u;  // "empty" wait before a copy gave up
                     }
                 }
                 if (ok) {
                     ok = mbar_wait(smem_u32(&s_full[s]), ph_full[s]);
                     if (ok) ph_full[s] ^= 1u;
+                    else err_code = 0x20u;  // copy completion wait gave up
                 }
                 if (ok) {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll
-                    for (int t = 0; t < BK / 16; ++t) {
+                    const int nt = k_steps(kbeg + kb * BK, kend);
+                    for (int t = 0; t < nt; ++t) {
                         const uint64_t ad = smem_desc(a0 + t * 2 * (BM * 16), BM * 16, 128);
                         const uint64_t bd = smem_desc(b0 + t * 2 * (bn * 16), bn * 16, 128);
                         mma_bf16(tmem, ad, bd, idesc, (kb > 0 || t > 0) ? 1u : 0u);
@@ -307,8 +321,8 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll
-            for (int t = 0; t < BK / 16; ++t) {
+            const int nt = k_steps(k0, kend);
+            for (int t = 0; t < nt; ++t) {
                 const uint64_t ad = smem_desc(a0 + t * 2 * (BM * 16), BM * 16, 128);
                 const uint64_t bd = smem_desc(b0 + t * 2 * (bn * 16), bn * 16, 128);
                 mma_bf16(tmem, ad, bd, idesc, (kb > 0 || t > 0) ? 1u : 0u);
@@ -323,21 +337,29 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
         // and, after an error, for any stage copy still in flight.
         if (issued > 0) {
             const int s = (issued - 1) & 1;
-            if (!mbar_wait(smem_u32(&s_empty[s]), ph_empty[s])) s_ok = 0;
+            if (!mbar_wait(smem_u32(&s_empty[s]), ph_empty[s])) {
+                s_ok = 0;
+                err_code |= 0x40u;  // last MMA commit wait gave up
+            }
         }
         if (TMA && loaded > issued) {
             for (int kb = issued; kb < loaded; ++kb) {
                 const int s = kb & 1;
-                if (!mbar_wait(smem_u32(&s_full[s]), ph_full[s])) s_ok = 0;
-                ph_full[s] ^= 1u;
+                if (!mbar_wait(smem_u32(&s_full[s]), ph_full[s])) {
+                    s_ok = 0;
+                    err_code |= 0x80u;  // drain of a copy in flight gave up
+                } else {
+                    ph_full[s] ^= 1u;
+                }
             }
         }
+        if (!s_ok && err_code == 0u) err_code = 0x08u;
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const bool ok = s_ok != 0;
     if (!ok) {
-        if (tid == 0 && g.err) atomicOr(g.err, 1u);
+        if (tid == 0 && g.err) atomicOr(g.err, 1u | err_code);
     } else {
         const int r = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);

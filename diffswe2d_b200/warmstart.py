@@ -327,8 +327,9 @@ class WarmStartNet:
         return loss
 
     def check_errors(self):
-        if int(self.err.item()) != 0:
-            raise RuntimeError("a tensor-core wait in nn_gemm_bf16 ran past its time limit")
+        code = int(self.err.item())
+        if code != 0:
+            raise RuntimeError(f"a bounded wait in nn_gemm_bf16 ran past its time limit (code {code:#x})")
 
     def predict_controls(self, gauges_eta: torch.Tensor, batch: int = 256) -> torch.Tensor:
         """Spline control values [N, controls] (metres) for gauge series
