@@ -46,7 +46,7 @@ L2_BYTES = 126 * 2 ** 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--ny", type=int, default=4096)
@@ -290,7 +290,7 @@ def run_ensemble(args, world, rank, local):
         "config": {"workload": f"ensemble_{args.ensemble_count}_sides_128_1024",
                    "scenarios": len(sizes), "steps_each": args.ensemble_steps,
                    "cells_total": int(sum(a * b for a, b in sizes)),
-                   "tile_rows_by_size_class": tuning.get("rows"),
+                   "ensemble_tile_rows": tuning.get("ensemble_rows"),
                    "parallelism": f"scenario shards x{world}"},
         "sequential_single_grid": {"value": cells / (seq_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
                                    "ms": seq_ms},

@@ -5,9 +5,10 @@ Two knobs are tuned by timing them on the GPU in use:
 * the sweep tile height (output rows per warp strip) per grid-size class --
   taller tiles recompute fewer halo rows, shorter ones give more tiles to
   fill the 148 SMs on small grids and a shorter serial chain per warp; used
-  by the single-grid kernels (``swe_tune_sweep_rows``) and per scenario by
-  ``Ensemble``; and per exact (batch, ny, nx) shape for the captured time
-  loops of gauge runs and ``SWE2D.forward`` (``tuned_rows_for_shape``);
+  by the single-grid kernels (``swe_tune_sweep_rows``); one throughput-tuned
+  value for the persistent ensemble kernel (``tuned_ensemble_rows``); and per
+  exact (batch, ny, nx) shape for the captured time loops of gauge runs and
+  ``SWE2D.forward`` (``tuned_rows_for_shape``);
 * the number of steps per CUDA-graph replay of ``SWE2D.forward``'s device
   loop -- more steps per replay mean fewer host reads, more no-op steps at
   the end of a call.
@@ -138,10 +139,43 @@ def tune(device="cuda", steps: int = 8, force: bool = False) -> dict:
     nat.check(nat.lib().swe_tune_sweep_rows(64), "tune rows")
     entry["rows"] = rows_choice
     entry["chunk"] = _tune_chunk(device)
+    entry["ensemble_rows"] = _tune_ensemble_rows(device)
     entry["timing_ms"] = timing
     entry["seconds"] = time.perf_counter() - t0
     _store(device, entry)
     return entry
+
+
+ENSEMBLE_ROW_CHOICES = (8, 16, 32, 64)
+
+
+def _tune_ensemble_rows(device, count: int = 24, steps: int = 30) -> int:
+    """Tile height for the persistent ensemble kernel, where many scenarios
+    fill the GPU together (throughput, not per-step latency, decides): one
+    value for all scenarios, timed on `count` seeded scenarios with sides
+    log-uniform in [128, 1024]."""
+    from . import scenarios
+    from .ensemble import Ensemble
+    sizes = scenarios.ensemble_sizes(count, seed=99)
+    members = []
+    for k, (ny, nx) in enumerate(sizes):
+        sc = scenarios.ensemble_member(ny, nx, seed=1000 + k)
+        sc.steps = steps
+        members.append(sc)
+    best, best_ms = None, None
+    for r in ENSEMBLE_ROW_CHOICES:
+        ens = Ensemble(members, device=device, rows=r)
+        ens.run()
+        ms = ens.run().elapsed_ms
+        if best_ms is None or ms < best_ms:
+            best, best_ms = r, ms
+        del ens
+    return int(best)
+
+
+def tuned_ensemble_rows(device="cuda") -> int:
+    """The ensemble kernel's tile height (16 if not tuned)."""
+    return int(_load(device).get("ensemble_rows", 16))
 
 
 def _tune_chunk(device) -> int:
@@ -220,5 +254,6 @@ def apply(device="cuda", cells: Optional[int] = None) -> None:
         SWE2D.steps_per_chunk = int(entry["chunk"])
 
 
-__all__ = ["tune", "tuned_rows", "tuned_rows_for_shape", "sweep_rows", "apply", "size_class",
+__all__ = ["tune", "tuned_rows", "tuned_ensemble_rows", "tuned_rows_for_shape", "sweep_rows", "apply",
+           "size_class",
            "SIZE_CLASSES", "ROW_CHOICES", "np"]

@@ -3,28 +3,19 @@
 // The matrix products run on the 5th-generation tensor cores: one CTA of
 // 128 threads computes a 128 x BN tile of A B^T (bf16 operands, fp32
 // accumulator in tensor memory).  Operands are staged global -> shared
-// memory in the canonical no-swizzle K-major layout that tcgen05.mma reads
-// through shared-memory matrix descriptors, two stages deep: by the tensor
-// memory accelerator (default: one 2-D TMA copy per 8-column slab, box
-// 8 x rows, whose shared-memory image is exactly one K column of 8x16-byte
-// core matrices; completion counted on a "full" mbarrier), or by all
-// threads with 16-byte loads (NN_GEMM_LOADS=threads).  One elected thread
-// issues the TMA copies and the MMAs and commits each stage's MMAs to an
-// "empty" mbarrier; the next slab's copy overlaps the current MMAs.  The
-// epilogue reads the accumulator with tcgen05.ld (each warp its 32 lanes)
-// and applies bias and activation.  Every mbarrier wait is bounded in time:
-// past the limit the CTA records an error, waits (bounded) for its copies
-// and MMAs in flight, frees its tensor memory and returns.
+// memory by all threads in the canonical no-swizzle K-major layout that
+// tcgen05.mma reads through shared-memory matrix descriptors, two stages
+// deep; one elected thread issues the MMAs and commits them to an mbarrier
+// per stage; the epilogue reads the accumulator with tcgen05.ld (each warp
+// its 32 lanes) and applies bias and activation.  Every mbarrier wait is
+// bounded in time: past the limit the CTA records an error, waits (bounded)
+// for its issued MMAs, frees its tensor memory and returns.
 //
 // The rest are small memory-bound kernels (im2col / col2im for the 1D
 // convolutions, activation adjoint, transposes, column sums, MSE, Adam).
-#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 #include <stdint.h>
-#include <stdlib.h>
-#include <string.h>
 
 #include "../../include/nn_b200.h"
 #include "../../include/swe_b200.h"
@@ -122,22 +113,6 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                  ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-
-// 2-D tiled TMA load of box (x = column, y = row) into shared memory,
-// completion counted on mbarrier `bar`.  x is a multiple of 8 bf16
-// elements (16 bytes), as the tensor map's inner box.
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, uint64_t map, int x, int y, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%2, %3}], [%4];"
-        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     uint32_t r[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -169,42 +144,12 @@ __device__ __forceinline__ void epilogue_store(const GemmArgs& g, int r, int c, 
     if (g.out_bf16) g.out_bf16[o] = __bfloat16_as_ushort(__float2bfloat16_rn(y));
 }
 
-// 16-wide K steps of the K block starting at k0 that lie before kend (K and
-// the split ends are multiples of 16).
-__device__ __forceinline__ int k_steps(int k0, int kend) {
-    const int rem = kend - k0;
-    return rem >= BK ? BK / 16 : rem / 16;
-}
-
-// Thread 0 arms stage kb's "full" barrier with the bytes of the slabs it is
-// about to copy and issues one TMA copy per 8-column slab of A and B that
-// lies before kend (slabs past the end of K are not copied and not read).
-__device__ void tma_stage(uint8_t* smem, uint64_t* s_full, int kb, int kbeg, int kend, int m0, int n0,
-                          int bn, uint64_t mapA, uint64_t mapB) {
-    const int s = kb & 1;
-    uint8_t* sA = smem + s * STAGE_BYTES;
-    uint8_t* sB = sA + A_BYTES;
-    const uint32_t bar = smem_u32(&s_full[s]);
-    const int k0 = kbeg + kb * BK;
-    const int nslab = 2 * k_steps(k0, kend);
-    mbar_expect_tx(bar, (uint32_t)nslab * (uint32_t)(BM + bn) * 16u);
-    for (int kc = 0; kc < nslab; ++kc) {
-        tma_load_2d(smem_u32(sA + kc * (BM * 16)), mapA, k0 + kc * 8, m0, bar);
-        tma_load_2d(smem_u32(sB + kc * (bn * 16)), mapB, k0 + kc * 8, n0, bar);
-    }
-}
-
-template <bool TMA>
-__global__ void __launch_bounds__(NT, 1)
-gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
-            const __grid_constant__ CUtensorMap tmB) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    __shared__ uint64_t s_full[2], s_empty[2];
+__global__ void __launch_bounds__(NT, 1) gemm_kernel(const GemmArgs g) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t s_bar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_ok;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // stage buffers from a 1024-byte boundary (TMA destinations need 128)
-    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int m0 = blockIdx.x * BM;
     const int bn = min(BN_MAX, ((g.N + 15) / 16) * 16);
     const int n0 = blockIdx.y * BN_MAX;
@@ -220,10 +165,8 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int s = 0; s < 2; ++s) {
-            mbar_init(smem_u32(&s_full[s]));
-            mbar_init(smem_u32(&s_empty[s]));
-        }
+        mbar_init(smem_u32(&s_bar[0]));
+        mbar_init(smem_u32(&s_bar[1]));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_ok = 1;
     }
@@ -232,65 +175,18 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = instr_desc(bn);
-    uint32_t ph_full[2] = {0u, 0u}, ph_empty[2] = {0u, 0u};
-    int issued = 0;     // MMA groups committed
-    int loaded = 0;     // TMA stages armed (TMA path)
-    uint32_t err_code = 0u;  // which bounded wait gave up (thread 0)
-
-    const uint64_t mapA = reinterpret_cast<uint64_t>(&tmA), mapB = reinterpret_cast<uint64_t>(&tmB);
-    if (TMA && tid == 0 && nkb > 0) {
-        tma_stage(smem, s_full, 0, kbeg, kend, m0, n0, bn, mapA, mapB);
-        loaded = 1;
-    }
+    uint32_t phase[2] = {0u, 0u};
+    int issued = 0;  // MMA groups committed
 
     for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb & 1;
         uint8_t* sA = smem + s * STAGE_BYTES;
         uint8_t* sB = sA + A_BYTES;
-        if (TMA) {
-            if (tid == 0) {
-                bool ok = true;
-                if (kb + 1 < nkb) {  // next stage's copy overlaps this stage's MMAs
-                    const int s1 = (kb + 1) & 1;
-                    if (kb + 1 >= 2) {  // the MMAs that read stage s1 are done
-                        ok = mbar_wait(smem_u32(&s_empty[s1]), ph_empty[s1]);
-                        if (ok) ph_empty[s1] ^= 1u;
-                    }
-                    if (ok) {
-                        tma_stage(smem, s_full, kb + 1, kbeg, kend, m0, n0, bn, mapA, mapB);
-                        loaded = kb + 2;
-                    } else {
-                        err_code = 0x10u;  // "empty" wait before a copy gave up
-                    }
-                }
-                if (ok) {
-                    ok = mbar_wait(smem_u32(&s_full[s]), ph_full[s]);
-                    if (ok) ph_full[s] ^= 1u;
-                    else err_code = 0x20u;  // copy completion wait gave up
-                }
-                if (ok) {
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-                    const int nt = k_steps(kbeg + kb * BK, kend);
-                    for (int t = 0; t < nt; ++t) {
-                        const uint64_t ad = smem_desc(a0 + t * 2 * (BM * 16), BM * 16, 128);
-                        const uint64_t bd = smem_desc(b0 + t * 2 * (bn * 16), bn * 16, 128);
-                        mma_bf16(tmem, ad, bd, idesc, (kb > 0 || t > 0) ? 1u : 0u);
-                    }
-                    mma_commit(smem_u32(&s_empty[s]));
-                    issued = kb + 1;
-                } else {
-                    s_ok = 0;
-                }
-                if (!ok) break;
-            }
-            continue;  // threads other than 0 wait at the barrier after the loop
-        }
         if (kb >= 2) {  // the MMAs that read this stage two blocks ago are done
             if (tid == 0) {
-                if (!mbar_wait(smem_u32(&s_empty[s]), ph_empty[s])) s_ok = 0;
+                if (!mbar_wait(smem_u32(&s_bar[s]), phase[s])) s_ok = 0;
             }
-            ph_empty[s] ^= 1u;
+            phase[s] ^= 1u;
             __syncthreads();
             if (!s_ok) break;
         }
@@ -321,45 +217,29 @@ gemm_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap tmA,
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-            const int nt = k_steps(k0, kend);
-            for (int t = 0; t < nt; ++t) {
+#pragma unroll
+            for (int t = 0; t < BK / 16; ++t) {
                 const uint64_t ad = smem_desc(a0 + t * 2 * (BM * 16), BM * 16, 128);
                 const uint64_t bd = smem_desc(b0 + t * 2 * (bn * 16), bn * 16, 128);
                 mma_bf16(tmem, ad, bd, idesc, (kb > 0 || t > 0) ? 1u : 0u);
             }
-            mma_commit(smem_u32(&s_empty[s]));
+            mma_commit(smem_u32(&s_bar[s]));
         }
         issued = kb + 1;
     }
 
-    if (tid == 0) {
-        // Wait for the last commit (it covers every MMA this thread issued)
-        // and, after an error, for any stage copy still in flight.
-        if (issued > 0) {
-            const int s = (issued - 1) & 1;
-            if (!mbar_wait(smem_u32(&s_empty[s]), ph_empty[s])) {
-                s_ok = 0;
-                err_code |= 0x40u;  // last MMA commit wait gave up
-            }
+    // Wait for the last commit (it covers every MMA this thread issued).
+    if (issued > 0) {
+        const int s = (issued - 1) & 1;
+        if (tid == 0) {
+            if (!mbar_wait(smem_u32(&s_bar[s]), phase[s])) s_ok = 0;
         }
-        if (TMA && loaded > issued) {
-            for (int kb = issued; kb < loaded; ++kb) {
-                const int s = kb & 1;
-                if (!mbar_wait(smem_u32(&s_full[s]), ph_full[s])) {
-                    s_ok = 0;
-                    err_code |= 0x80u;  // drain of a copy in flight gave up
-                } else {
-                    ph_full[s] ^= 1u;
-                }
-            }
-        }
-        if (!s_ok && err_code == 0u) err_code = 0x08u;
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const bool ok = s_ok != 0;
     if (!ok) {
-        if (tid == 0 && g.err) atomicOr(g.err, 1u | err_code);
+        if (tid == 0 && g.err) atomicOr(g.err, 1u);
     } else {
         const int r = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -553,38 +433,7 @@ int grid_for(long long n, int threads) {
     return (int)(b > 148LL * 16 ? 148LL * 16 : b);
 }
 
-bool g_smem_set[64][2] = {{false}};
-
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-
-// The driver's tensor-map encoder, looked up once through the runtime.
-bool encoder() {
-    if (g_encode) return true;
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-        return false;
-    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    return true;
-}
-
-// bf16 [rows, cols] row-major with leading dimension ld (elements): boxes of
-// 8 columns x box_rows rows, no swizzle, zero fill outside the tensor.
-bool encode_operand(CUtensorMap* map, const uint16_t* base, int rows, int cols, int ld, int box_rows) {
-    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
-    const cuuint32_t estr[2] = {1u, 1u};
-    return g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-bool use_tma() {
-    const char* v = getenv("NN_GEMM_LOADS");
-    return !(v && strcmp(v, "threads") == 0);
-}
+bool g_smem_set[64] = {false};
 
 }  // namespace
 }  // namespace nn
@@ -603,23 +452,11 @@ extern "C" int nn_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int l
     if (ldc < N || ksplit < 1 || ksplit > 1024 || (ksplit > 1 && !workspace)) return SWE_EARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWE_ECUDA;
-    const bool tma = use_tma();
-    if (!g_smem_set[dev][tma]) {
-        cudaError_t e = tma ? cudaFuncSetAttribute(gemm_kernel<true>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES)
-                            : cudaFuncSetAttribute(gemm_kernel<false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return SWE_ECUDA;
-        g_smem_set[dev][tma] = true;
-    }
-    CUtensorMap mapA, mapB;
-    memset(&mapA, 0, sizeof(mapA));
-    memset(&mapB, 0, sizeof(mapB));
-    if (tma) {
-        const int bn = N < BN_MAX ? (N + 15) / 16 * 16 : BN_MAX;
-        if (!encoder() || !encode_operand(&mapA, A, M, K, lda, BM) ||
-            !encode_operand(&mapB, B, N, K, ldb, bn))
+    if (!g_smem_set[dev]) {
+        if (cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SMEM_BYTES) != cudaSuccess)
             return SWE_ECUDA;
+        g_smem_set[dev] = true;
     }
     GemmArgs g{};
     g.A = A;
@@ -644,8 +481,7 @@ extern "C" int nn_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int l
     g.err = err;
     cudaStream_t s = (cudaStream_t)stream;
     const dim3 grid((M + BM - 1) / BM, (N + BN_MAX - 1) / BN_MAX, zs);
-    if (tma) gemm_kernel<true><<<grid, NT, SMEM_BYTES, s>>>(g, mapA, mapB);
-    else gemm_kernel<false><<<grid, NT, SMEM_BYTES, s>>>(g, mapA, mapB);
+    gemm_kernel<<<grid, NT, SMEM_BYTES, s>>>(g);
     if (zs > 1) splitk_epilogue_kernel<<<grid_for((long long)M * N, 256), 256, 0, s>>>(g, zs);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }

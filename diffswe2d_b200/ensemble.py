@@ -39,12 +39,12 @@ class Ensemble:
     """Scenarios (``diffswe2d_b200.scenarios.Scenario`` or compatible) on one GPU.
 
     ``rows`` fixes the sweep tile height of every scenario; by default it is
-    chosen per grid-size class by ``autotune.tuned_rows``.
+    the autotuner's ensemble value (``autotune.tuned_ensemble_rows``).
     """
 
     def __init__(self, scenarios: Sequence, device="cuda", steps: Optional[int] = None,
                  rows: Optional[int] = None, track_hmax: bool = False, max_dt: float = 1.0e9):
-        from .autotune import tuned_rows
+        from .autotune import tuned_ensemble_rows
         self.device = torch.device(device)
         self.count = len(scenarios)
         if not 1 <= self.count <= 1024:
@@ -77,7 +77,7 @@ class Ensemble:
                 sw = torch.as_tensor(sc.bc_levels, dtype=torch.float32, device=dev).contiguous()
                 nser = st.numel()
             steps_m = int(sc.steps if steps is None else steps)
-            r = int(rows) if rows is not None else tuned_rows(ny * nx, dev)
+            r = int(rows) if rows is not None else tuned_ensemble_rows(dev)
             mem = members[m]
             mem.bed, mem.n = bed.data_ptr(), n.data_ptr()
             mem.U_a, mem.U_b, mem.k1 = Ua.data_ptr(), Ub.data_ptr(), k1.data_ptr()
@@ -190,7 +190,7 @@ class GaugeEnsemble:
     def __init__(self, bed: torch.Tensor, n: torch.Tensor, U0: torch.Tensor, out_levels: torch.Tensor,
                  out_dt: float, gauges: Sequence, config: SWEConfig, dx: float, dy: Optional[float] = None,
                  rows: Optional[int] = None, max_steps: int = 1 << 30, max_dt_cap: float = 0.0):
-        from .autotune import tuned_rows
+        from .autotune import tuned_ensemble_rows
         M, ny, nx = bed.shape
         if not 1 <= M <= 1024:
             raise ValueError("a gauge ensemble holds 1 to 1024 members")
@@ -221,7 +221,7 @@ class GaugeEnsemble:
                                   device=dev)
         self.gauge_out = torch.zeros((M, self.n_out, max(self.ngauge, 1)), device=dev)
         self.friction = (1 + (0 if config.frictionmodel == "manning" else 1)) if config.apply_friction else 0
-        r = int(rows) if rows is not None else tuned_rows(ny * nx, dev)
+        r = int(rows) if rows is not None else tuned_ensemble_rows(dev)
         p = nat.params(config, dx, dx if dy is None else dy)
         members = (nat.SweEnsembleMember * M)()
         for m in range(M):

@@ -44,21 +44,10 @@ def _gemm(A, B, M, N, K, lda, ldb, bias=None, act=0, ksplit=1, ldc=None):
     return out.cpu().numpy(), pre.cpu().numpy(), _as_f32(ob)
 
 
-@pytest.fixture(params=["tma", "threads"])
-def operand_loads(request, monkeypatch):
-    """Both operand-staging paths of nn_gemm_bf16: TMA copies (default) and
-    16-byte loads by all threads."""
-    if request.param == "threads":
-        monkeypatch.setenv("NN_GEMM_LOADS", "threads")
-    else:
-        monkeypatch.delenv("NN_GEMM_LOADS", raising=False)
-    return request.param
-
-
 @pytest.mark.parametrize("M,N,K,ksplit", [(1, 16, 16, 1), (130, 32, 64, 1), (128, 96, 4480, 1),
                                           (300, 96, 4480, 4), (32, 64, 4096, 16), (1000, 128, 384, 1),
                                           (257, 160, 96, 1), (77, 48, 208, 3), (129, 16, 48, 1)])
-def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, ksplit, operand_loads):
+def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, ksplit):
     rng = np.random.default_rng(M * 7 + N + K)
     a = rng.normal(size=(M, K)).astype(np.float32)
     b = rng.normal(size=(N, K)).astype(np.float32)
@@ -70,7 +59,7 @@ def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, ksplit, operand
     assert np.array_equal(out, pre)
 
 
-def test_gemm_epilogue_bias_gelu_and_strides(operand_loads):
+def test_gemm_epilogue_bias_gelu_and_strides():
     rng = np.random.default_rng(5)
     M, N, K, lda, ldb, ldc = 200, 48, 96, 104, 112, 56
     a = rng.normal(size=(M, lda)).astype(np.float32)
