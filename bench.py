@@ -39,6 +39,11 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 BYTES_PER_CELL_UPDATE = 32  # read h,hu,hv,z,n once, write h,hu,hv once
+# DRAM bytes per cell of one stage-2 launch from the ncu capture of
+# profiles/sweep_kernels_runup_3072.md (302.1 MB read + 95.9 MB written over
+# 3072^2 cells); traffic grows with the cells, so a launch of the bench's grid
+# moves this many bytes per cell.
+STAGE2_DRAM_BYTES_PER_CELL = (302.098944e6 + 95.926016e6) / (3072 * 3072)
 STAGE2_BYTES_PER_CELL = 44  # stage-2 kernel: read U, k1, z, n; write U
 L2_BYTES = 126 * 2 ** 20
 
@@ -585,7 +590,9 @@ def main():
                    "tuned_rows_by_size_class": tuning.get("rows")},
         "roofline": {"bound": "hbm", "kernel": "stage2 (predictor+tendency+corrector+friction)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": STAGE2_DRAM_BYTES_PER_CELL * cells,
+                     "traffic_source": "ncu dram__bytes_read+write of stage 2 at 3072^2, scaled by cells",
+                     "peak_kind": peak_kind,
                      "bytes_per_cell": STAGE2_BYTES_PER_CELL,
                      "stage1_ms": s1_avg, "stage2_ms": s2_avg,
                      "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak,
