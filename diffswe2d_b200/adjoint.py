@@ -112,17 +112,20 @@ class AdjointStepper:
                 nat.ptr(P_out), self.st)
         nat.check(rc, ("adjoint corrector", "adjoint predictor", "adjoint predictor")[mode])
 
-    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n):
+    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n, K1=None):
         """lam_U += (d U_new / d U)^T lam_out and lam_n += the roughness
         adjoint (when friction is on) for the step at input state U with
         level vector lv and time step dt (a float, or a one-element device
         tensor); returns the level adjoint's partial sums
         [2, B * LEVEL_BLOCKS] (their sum per batch member is that member's
-        level adjoint)."""
+        level adjoint).  K1, if given, is the step's stage-1 tendency kept
+        from the forward recompute (else it is recomputed here)."""
         lib, st, p, B, ny, nx = self.lib, self.st, self.p, self.B, self.ny, self.nx
-        K1, K2, P, lam_k, lam_P = self.K1, self.K2, self.P, self.lam_k, self.lam_P
+        K2, P, lam_k, lam_P = self.K2, self.P, self.lam_k, self.lam_P
         # recompute the step's stage intermediates (solver.py:613-646)
-        self._tendency(U, lv, K1)
+        if K1 is None:
+            K1 = self.K1
+            self._tendency(U, lv, K1)
         self._pointwise(2, U, K1, dt, None, None, None, P)
         self._tendency(P, lv, K2)
         lam_P.zero_()

@@ -94,11 +94,14 @@ class GaugeRunWorkspace:
             nat.ptr(self.step_code), nat.stream_handle(self.dev))
         nat.check(rc, "gauge-run clock")
 
-    def _step(self, src, dst):
+    def _step(self, src, dst, k1=None):
+        """One clocked step src -> dst; its stage-1 tendency goes to k1 (the
+        shared scratch if None) and the clock advances."""
+        k1 = self.scratch if k1 is None else k1
         rc = nat.lib().swe_step_clocked_f32(
             3, nat.ptr(src), nat.ptr(self.bed), self.bed.shape[0], nat.ptr(self.n), self.n.shape[0],
             self.B, self.ny, self.nx, self.params, nat.ptr(self.lv), self.levelB, nat.ptr(self.clock),
-            None, nat.FORCING_NONE, 1, nat.ptr(self.scratch), nat.ptr(self.red), nat.ptr(dst), None,
+            None, nat.FORCING_NONE, 1, nat.ptr(k1), nat.ptr(self.red), nat.ptr(dst), None,
             nat.stream_handle(self.dev))
         nat.check(rc, "gauge-run step")
         self._tick(dst)
@@ -171,9 +174,12 @@ class GaugeRunWorkspace:
 
     # ------------------------------------------------------------ backward
     def _recompute_segment(self, j: int, s0: int, s1: int):
-        """States entering steps s0 .. s1-1 into self.seg[0 .. s1-s0-1]."""
+        """States entering steps s0 .. s1-1 into self.seg[0 .. s1-s0-1] and
+        their stage-1 tendencies into self.seg_k1 (the adjoint reuses them:
+        the same kernel on the same state and level gives the same bits)."""
         if self.seg is None:
             self.seg = [torch.empty_like(self.bufs[0]) for _ in range(self.k + 1)]
+            self.seg_k1 = [torch.empty_like(self.bufs[0]) for _ in range(self.k)]
         self.seg[0].copy_(self.ckpts[j])
         self._set_clock(replay=1, replay_end=s1, steps=s0, active=0)
         self._tick(self.seg[0])
@@ -182,7 +188,7 @@ class GaugeRunWorkspace:
             g = torch.cuda.CUDAGraph()
             with sweep_rows(self.rows), torch.cuda.graph(g):
                 for i in range(self.k):
-                    self._step(self.seg[i], self.seg[i + 1])
+                    self._step(self.seg[i], self.seg[i + 1], self.seg_k1[i])
             self.replay_graph = g
         self.replay_graph.replay()
 
@@ -213,7 +219,8 @@ class GaugeRunWorkspace:
                 nat.ptr(self.g_gauge), self.n_out, self.record_cap, st)
             nat.check(rc, "gauge-run adjoint setup")
             lam_out.zero_()
-            part = stp(self.seg[i], self.lv_cur, self.dt_cur, lam_in, lam_out, self.lam_n)
+            part = stp(self.seg[i], self.lv_cur, self.dt_cur, lam_in, lam_out, self.lam_n,
+                       K1=self.seg_k1[i])
             rc = lib.swe_gauge_adjoint_post_f32(
                 nat.ptr(self.cursor), nat.ptr(self.step_code), nat.ptr(part), 2, self.B,
                 LEVEL_BLOCKS, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)
