@@ -347,7 +347,8 @@ def run_inversion(args, world, rank, local):
         e1.record()
         torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / args.steps
-    steps = [w.last_steps for w in _WORKSPACES.values()][0]
+    ws = list(_WORKSPACES.values())[0]
+    steps = ws.last_steps
     cells = args.inv_cases * gy * gx * steps
     line = {
         "metric": "adjoint inversion: seconds per Adam iteration (config 3)",
@@ -357,7 +358,9 @@ def run_inversion(args, world, rank, local):
         "config": {"workload": f"runup_inversion_{gy}x{gx}", "dx": gdx, "cases": args.inv_cases,
                    "controls": 16, "gauges": 6, "dt_out": 0.02, "duration_s": args.inv_duration,
                    "lr": 0.002,
-                   "solver_steps_per_run": steps, "checkpoint_every": 128,
+                   "solver_steps_per_run": steps, "checkpoint_every": ws.k,
+                   "backward_states": "kept from the forward pass" if ws.stored
+                   else "recomputed from checkpoints",
                    "l2": "per-iteration working set (states, checkpoints, face buffers) > L2"},
         "forward_plus_adjoint_mcell_per_s": cells / (ms * 1e-3) / 1e6,
         "loss": float(loss), "clocks": clk.summary(),

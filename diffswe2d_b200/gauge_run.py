@@ -19,6 +19,10 @@ state after each call, autograd through everything (optionally
   recomputed from its checkpoint in replay mode (bit for bit the forward's
   states), then the hand-written step adjoint runs in reverse over the
   segment with the gauge cotangents injected at the end of each interval.
+  When the whole trajectory fits in device memory (``store_states``, decided
+  by free memory by default), the forward pass keeps every step's output
+  state and stage-1 tendency instead, and the backward pass copies a
+  segment's states into place rather than recomputing them.
 
 Gradients flow to the initial state, the per-interval levels and the
 roughness field, as through the reference's loop (dt detached).
@@ -43,7 +47,8 @@ class GaugeRunWorkspace:
 
     def __init__(self, model, B: int, ny: int, nx: int, dev, levelB: int, n_out: int,
                  gauges: Sequence[Tuple[int, int]], graph_steps: int = GRAPH_STEPS,
-                 checkpoint_every: int = CHECKPOINT_EVERY, record_cap: Optional[int] = None):
+                 checkpoint_every: int = CHECKPOINT_EVERY, record_cap: Optional[int] = None,
+                 store_states: Optional[bool] = None):
         if graph_steps < 2 or graph_steps % 2:
             raise ValueError("graph_steps must be even and >= 2")
         if checkpoint_every < graph_steps or checkpoint_every % graph_steps:
@@ -82,6 +87,12 @@ class GaugeRunWorkspace:
         self.last_steps = 0
         self.generation = 0
         self.stepper = None
+        # full-trajectory storage (None: when free device memory allows)
+        self.store_mode = store_states
+        self.ring = self.ring_k1 = None
+        self.fwd_store_graph = None
+        self.store, self.store_k1 = [], []
+        self.stored = False
         from .autotune import tuned_rows_for_shape
         self.rows = tuned_rows_for_shape(B, ny, nx, dev)
 
@@ -149,6 +160,18 @@ class GaugeRunWorkspace:
                 for s in range(self.G):
                     self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
             self.fwd_graph = g
+        storing = self.store_mode is not False
+        if storing and self.fwd_store_graph is None:
+            from .autotune import sweep_rows
+            self.ring = torch.empty((self.G,) + tuple(self.bufs[0].shape), device=self.dev)
+            self.ring_k1 = torch.empty_like(self.ring)
+            g = torch.cuda.CUDAGraph()
+            with sweep_rows(self.rows), torch.cuda.graph(g):
+                for s in range(self.G):
+                    self._step(self.bufs[0] if s == 0 else self.ring[s - 1], self.ring[s],
+                               self.ring_k1[s])
+                self.bufs[0].copy_(self.ring[self.G - 1])
+            self.fwd_store_graph = g
         per_ckpt = self.k // self.G
         replay = 0
         while True:
@@ -157,11 +180,14 @@ class GaugeRunWorkspace:
                 if j == len(self.ckpts):
                     self.ckpts.append(torch.empty_like(self.bufs[0]))
                 self.ckpts[j].copy_(self.bufs[0])
-            self.fwd_graph.replay()
+            (self.fwd_store_graph if storing else self.fwd_graph).replay()
+            if storing:
+                storing = self._keep_replay(replay)
             replay += 1
             c = self._read_clock()
             if c.base.state != nat.CLOCK_RUNNING:
                 break
+        self.stored = storing
         if c.base.state == nat.CLOCK_FAILED:
             self.model._raise_on_status(int(c.base.dt_status), float(c.base.last_dt))
         if c.base.state == nat.CLOCK_MAXSTEPS:
@@ -173,13 +199,51 @@ class GaugeRunWorkspace:
         return self.gauge_out[..., : self.ngauge], self.bufs[0]
 
     # ------------------------------------------------------------ backward
+    def _keep_replay(self, r: int) -> bool:
+        """Copy replay r's step outputs and tendencies into the store; False
+        (stop storing) when the store would leave too little device memory
+        or storage is switched off."""
+        if r == len(self.store):
+            need = 2 * self.ring.numel() * 4
+            if self.store_mode is None:
+                free, total = torch.cuda.mem_get_info(self.dev)
+                if free - need < max(8 << 30, int(0.15 * total)):
+                    return False
+            self.store.append(torch.empty_like(self.ring))
+            self.store_k1.append(torch.empty_like(self.ring_k1))
+        self.store[r].copy_(self.ring)
+        self.store_k1[r].copy_(self.ring_k1)
+        return True
+
+    def _copy_steps(self, dst, d0: int, chunks, s0: int, n: int):
+        """dst[d0 : d0+n] = step items s0 .. s0+n-1 of a store kept in chunks
+        of graph_steps items."""
+        while n > 0:
+            c, o = divmod(s0, self.G)
+            m = min(n, self.G - o)
+            dst[d0:d0 + m].copy_(chunks[c][o:o + m])
+            d0, s0, n = d0 + m, s0 + m, n - m
+
+    def _stored_segment(self, j: int, s0: int, s1: int):
+        """The segment's states and stage-1 tendencies copied from the store."""
+        self._alloc_segment()
+        n = s1 - s0
+        self.seg[0].copy_(self.ckpts[j])
+        if n > 1:
+            self._copy_steps(self.seg, 1, self.store, s0, n - 1)  # outputs of s0 .. s1-2
+        self._copy_steps(self.seg_k1, 0, self.store_k1, s0, n)
+
+    def _alloc_segment(self):
+        if self.seg is None:
+            shape = tuple(self.bufs[0].shape)
+            self.seg = torch.empty((self.k + 1,) + shape, device=self.dev)
+            self.seg_k1 = torch.empty((self.k,) + shape, device=self.dev)
+
     def _recompute_segment(self, j: int, s0: int, s1: int):
         """States entering steps s0 .. s1-1 into self.seg[0 .. s1-s0-1] and
         their stage-1 tendencies into self.seg_k1 (the adjoint reuses them:
         the same kernel on the same state and level gives the same bits)."""
-        if self.seg is None:
-            self.seg = [torch.empty_like(self.bufs[0]) for _ in range(self.k + 1)]
-            self.seg_k1 = [torch.empty_like(self.bufs[0]) for _ in range(self.k)]
+        self._alloc_segment()
         self.seg[0].copy_(self.ckpts[j])
         self._set_clock(replay=1, replay_end=s1, steps=s0, active=0)
         self._tick(self.seg[0])
@@ -260,7 +324,10 @@ class GaugeRunWorkspace:
     def _backward_segments(self, nseg, total):
         for j in range(nseg - 1, -1, -1):
             s0, s1 = j * self.k, min((j + 1) * self.k, total)
-            self._recompute_segment(j, s0, s1)
+            if self.stored:
+                self._stored_segment(j, s0, s1)
+            else:
+                self._recompute_segment(j, s0, s1)
             self.cursor.fill_(s1 - 1)
             count = s1 - s0
             if count < self.k:
@@ -323,7 +390,8 @@ _WORKSPACES = {}
 
 def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
               gauges: Sequence[Tuple[int, int]], max_dt_cap=None, max_steps: int = 1_000_000,
-              graph_steps: int = GRAPH_STEPS, checkpoint_every: int = CHECKPOINT_EVERY):
+              graph_steps: int = GRAPH_STEPS, checkpoint_every: int = CHECKPOINT_EVERY,
+              store_states: Optional[bool] = None):
     """Advance ``U0`` through ``n_out`` output intervals of ``out_dt``
     seconds; interval i runs exactly like ``model(U, t_end=out_dt,
     boundary_level=level_i)``, with level_i = ``levels[:, i]`` for levels
@@ -349,11 +417,11 @@ def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
     if not out_dt > 0:
         raise ValueError("out_dt must be positive")
     key = (id(model), B, ny, nx, str(U0.device), levelB, n_out, tuple(map(tuple, gauges)),
-           graph_steps, checkpoint_every)
+           graph_steps, checkpoint_every, store_states)
     ws = _WORKSPACES.get(key)
     if ws is None or ws.model is not model:
         ws = GaugeRunWorkspace(model, B, ny, nx, U0.device, levelB, n_out, gauges, graph_steps,
-                               checkpoint_every)
+                               checkpoint_every, store_states=store_states)
         _WORKSPACES.clear()
         _WORKSPACES[key] = ws
     levels_f = levels.to(dtype=torch.float32)
@@ -363,7 +431,8 @@ def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
                                            float(out_dt), max_dt_cap, int(max_steps))
         except _RecordFull as e:
             ws = GaugeRunWorkspace(model, B, ny, nx, U0.device, levelB, n_out, gauges, graph_steps,
-                                   checkpoint_every, record_cap=4 * e.steps)
+                                   checkpoint_every, record_cap=4 * e.steps,
+                                   store_states=store_states)
             _WORKSPACES.clear()
             _WORKSPACES[key] = ws
 

@@ -60,8 +60,10 @@ def test_forward_matches_chunked_forward_calls(B, shared):
     assert torch.equal(U, ref_U)
 
 
-@pytest.mark.parametrize("B", [1, 2])
-def test_gradients_match_chunked_checkpointed_autograd(B):
+@pytest.mark.parametrize("B,store", [(1, False), (2, False), (1, True), (2, True)])
+def test_gradients_match_chunked_checkpointed_autograd(B, store):
+    """Both backward modes: states recomputed from checkpoints (store=False)
+    and every step's state kept from the forward pass (store=True)."""
     out = []
     for mode in ("run", "chunks"):
         m, U0 = _model(B)
@@ -70,7 +72,8 @@ def test_gradients_match_chunked_checkpointed_autograd(B):
         levels = _levels(B, 8).requires_grad_(True)
         w = torch.linspace(-1.0, 2.0, B * 8 * len(GAUGES), device=DEV).view(B, 8, len(GAUGES))
         if mode == "run":
-            g, U = gauge_run(m, U0, levels, 0.2, GAUGES, graph_steps=2, checkpoint_every=6)
+            g, U = gauge_run(m, U0, levels, 0.2, GAUGES, graph_steps=2, checkpoint_every=6,
+                             store_states=store)
         else:
             g, U = _chunked(m, U0, levels, 0.2, grad=True)
         loss = (w * g).sum() + 1e-2 * (U * U).sum()
@@ -112,7 +115,8 @@ def test_backward_after_workspace_reuse_raises():
         g1.sum().backward()
 
 
-def test_bed_gradient_matches_chunked_autograd():
+@pytest.mark.parametrize("store", [False, True])
+def test_bed_gradient_matches_chunked_autograd(store):
     """gauge_run's bed (DEM correction) gradient equals the chunk-by-chunk
     forward_checkpointed gradient."""
     out = []
@@ -121,7 +125,8 @@ def test_bed_gradient_matches_chunked_autograd():
         m.dem_correction_parameter.requires_grad_(True)
         levels = _levels(1, 6)
         if mode == "run":
-            g, U = gauge_run(m, U0, levels, 0.2, GAUGES, graph_steps=2, checkpoint_every=6)
+            g, U = gauge_run(m, U0, levels, 0.2, GAUGES, graph_steps=2, checkpoint_every=6,
+                             store_states=store)
         else:
             g, U = _chunked(m, U0, levels, 0.2, grad=True)
         (g.sum() + 1e-2 * (U * U).sum()).backward()
