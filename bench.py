@@ -24,7 +24,6 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
-import math
 import os
 import statistics
 import subprocess

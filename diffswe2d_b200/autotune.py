@@ -24,7 +24,6 @@ import time
 from pathlib import Path
 from typing import Dict, Optional
 
-import numpy as np
 import torch
 
 from . import _native as nat
@@ -256,4 +255,4 @@ def apply(device="cuda", cells: Optional[int] = None) -> None:
 
 __all__ = ["tune", "tuned_rows", "tuned_ensemble_rows", "tuned_rows_for_shape", "sweep_rows", "apply",
            "size_class",
-           "SIZE_CLASSES", "ROW_CHOICES", "np"]
+           "SIZE_CLASSES", "ROW_CHOICES"]

@@ -14,7 +14,6 @@ gradient clipping of the reference script are optional and off by default.
 """
 from __future__ import annotations
 
-import math
 import time
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
@@ -297,4 +296,4 @@ def make_runup_problem(cases: int = 4, seed: int = 0, ny: int = 122, nx: int = 1
 
 
 __all__ = ["clamped_bspline_basis", "bounded_controls", "raw_from_controls", "InversionProblem",
-           "InversionResult", "invert", "gauge_rmse", "make_runup_problem", "RunupFamily", "math"]
+           "InversionResult", "invert", "gauge_rmse", "make_runup_problem", "RunupFamily"]

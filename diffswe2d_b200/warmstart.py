@@ -33,9 +33,8 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass
-from typing import List, Optional, Tuple
+from typing import List, Tuple
 
-import numpy as np
 import torch
 
 from . import _native as nat
@@ -354,5 +353,4 @@ def normalise_controls(values: torch.Tensor) -> torch.Tensor:
 
 
 __all__ = ["WarmStartNet", "architecture", "param_layout", "normalise_controls", "Conv", "Dense",
-           "SAMPLES", "GAUGES", "CONTROLS", "INPUT_SCALE", "CONTROL_MEAN", "CONTROL_SCALE", "np",
-           "Optional"]
+           "SAMPLES", "GAUGES", "CONTROLS", "INPUT_SCALE", "CONTROL_MEAN", "CONTROL_SCALE"]

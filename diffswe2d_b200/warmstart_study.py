@@ -21,8 +21,8 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
-from .inversion import RunupFamily, bounded_controls, invert, raw_from_controls
-from .warmstart import CONTROL_MEAN, CONTROL_SCALE, WarmStartNet, normalise_controls
+from .inversion import RunupFamily, invert, raw_from_controls
+from .warmstart import WarmStartNet, normalise_controls
 
 
 @dataclass
@@ -143,5 +143,4 @@ def _summary(res, extra_s: float) -> Dict:
     }
 
 
-__all__ = ["Dataset", "generate", "train", "compare", "TrainLog", "bounded_controls",
-           "CONTROL_MEAN", "CONTROL_SCALE"]
+__all__ = ["Dataset", "generate", "train", "compare", "TrainLog"]

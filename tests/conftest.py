@@ -4,7 +4,6 @@
 Everything else runs on the CPU: the oracle against the reference's golden
 outputs, the host-side logic, and the C ABI's exported symbols.
 """
-import os
 import sys
 from pathlib import Path
 

@@ -10,7 +10,6 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import normwise
 from oracle import OracleSWE
 
 from diffswe2d_b200 import SWE2D, SWEConfig

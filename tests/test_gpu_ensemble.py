@@ -5,7 +5,6 @@ launch; every scenario's final state, step count and simulated time must be
 bit for bit those of SWE2D.step run on that scenario by itself (its own CFL
 time steps and its own boundary series).
 """
-import numpy as np
 import pytest
 import torch
 

@@ -1,7 +1,6 @@
 """Inflow inversion through the adjoint on a small runup problem: the gauge
 misfit falls under Adam, and the gradient of the whole chunked simulation
 agrees with finite differences of the simulated misfit."""
-import numpy as np
 import pytest
 import torch
 

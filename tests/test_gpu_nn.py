@@ -11,7 +11,7 @@ import torch
 from warmstart_oracle import WarmStartOracle, bf16, col2im, gelu, gelu_grad, im2col, mse_grad
 
 from diffswe2d_b200 import _native as nat
-from diffswe2d_b200.warmstart import (INPUT_SCALE, WarmStartNet, architecture, param_layout)
+from diffswe2d_b200.warmstart import INPUT_SCALE, WarmStartNet, architecture
 
 pytestmark = pytest.mark.gpu
 DEV = "cuda:0"

@@ -16,7 +16,6 @@ test already.
 """
 import ctypes
 
-import numpy as np
 import pytest
 import torch
 
