@@ -362,7 +362,7 @@ def run_inversion(args, world, rank, local):
                    else "recomputed from checkpoints",
                    "l2": "per-iteration working set (states, checkpoints, face buffers) > L2"},
         "forward_plus_adjoint_mcell_per_s": cells / (ms * 1e-3) / 1e6,
-        "loss": float(loss), "clocks": clk.summary(),
+        "loss": float(loss.detach()), "clocks": clk.summary(),
         "gpu_launches": steps * 21 * args.steps,
     }
     if rank == 0:

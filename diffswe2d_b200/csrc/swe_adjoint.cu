@@ -419,7 +419,7 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
         const float ypw = shared_rcp(pw);
         cf = quot(num, pw, ypw);
         // d/d pw: -cf / pw ; d pw / d hpre = third * hpre^(third - 1)
-        const float dpw = k.third * (float)pow((double)hpre, (double)(k.third - 1.0f));
+        const float dpw = k.third * pow_pos(hpre, k.third - 1.0f);
         dcf_dpre = -quot(cf, pw, ypw) * dpw;
         dcf_dn = quot(k.g981 * (2.0f * nn), pw, ypw);
         h_pass = h >= k.fr_e;

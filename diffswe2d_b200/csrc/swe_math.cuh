@@ -435,11 +435,113 @@ SWE_HD State clean_and_limit(const State& o, State c, const SweConsts& k, bool p
     return r;
 }
 
-// x ** (float)(1/3) rounded to float (friction.py:66).  Evaluated in double
-// and rounded once; PyTorch's CPU pow agrees with this value on all but a
+SWE_HD uint64_t d2u(double x) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(x);
+#else
+    union { double d; uint64_t u; } t;
+    t.d = x;
+    return t.u;
+#endif
+}
+
+SWE_HD double u2d(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)x);
+#else
+    union { double d; uint64_t u; } t;
+    t.u = x;
+    return t.d;
+#endif
+}
+
+// x ** t for float x and t, as the double power x^t rounded once to float,
+// i.e. the value of (float)pow((double)x, (double)t), for positive normal x
+// and |t ln x| <= 700 (other arguments call pow itself).  The power is
+// exp(t ln x), evaluated in double with double-double intermediates:
+//   ln x = e ln 2 + ln m, m in [sqrt(1/2), sqrt(2)), ln m = 2 atanh(s) with
+//   s = (m - 1)/(m + 1) carried as s + s_lo (exact FMA remainder), and
+//   atanh(s)/s = sum s^2k/(2k+1) to k = 10 (|s| <= 0.1716: the first term
+//   left out is below 2^-60); ln 2 split in a 32-bit head (exact products
+//   with the exponent) and a tail (Cody and Waite, "Software Manual for the
+//   Elementary Functions", 1980);
+//   y = t ln x as a double-double, y = n ln 2 + r with n = rint(y / ln 2),
+//   |r| <= ln 2 / 2, exp(r) from its Taylor series to degree 13 (remainder
+//   below 2^-57), exp(y) = 2^n exp(r).
+// The double result is within about 2^-54 relative of x^t, so it rounds to
+// the same float as a correctly rounded double pow except for x^t within
+// that distance of a float rounding midpoint.  swe_selftest_arith_f32
+// (which = 4) compares it with CUDA's pow for every float x in a range.
+SWE_HD float pow_pos(float x, float t) {
+    const uint32_t xb = f2u(x);
+    if (xb - 0x00800000u >= 0x7f000000u) return (float)pow((double)x, (double)t);
+    constexpr double kLn2Hi = 0x1.62e42feep-1;              // 32 significant bits
+    constexpr double kLn2Lo = 0x1.a39ef35793c76p-33;        // ln 2 - kLn2Hi
+    constexpr double kInvLn2 = 0x1.71547652b82fep+0;        // 1 / ln 2
+    int e = (int)(xb >> 23) - 127;
+    uint32_t mb = (xb & 0x007fffffu) | 0x3f800000u;         // m in [1, 2)
+    if (mb > 0x3fb504f3u) {                                 // m > sqrt(2): halve it
+        mb -= 0x00800000u;
+        e += 1;
+    }
+    const double m = (double)u2f(mb);
+    const double num = m - 1.0, den = m + 1.0;              // both exact
+    const double inv = 1.0 / den;
+    const double s = num * inv;
+    const double s_lo = fma(-s, den, num) * inv;            // num/den = s + s_lo
+    const double s2 = s * s;
+    double q = 1.0 / 21;
+    q = fma(q, s2, 1.0 / 19);
+    q = fma(q, s2, 1.0 / 17);
+    q = fma(q, s2, 1.0 / 15);
+    q = fma(q, s2, 1.0 / 13);
+    q = fma(q, s2, 1.0 / 11);
+    q = fma(q, s2, 1.0 / 9);
+    q = fma(q, s2, 1.0 / 7);
+    q = fma(q, s2, 1.0 / 5);
+    q = fma(q, s2, 1.0 / 3);
+    // ln m = a_hi + a_lo
+    const double a_hi = 2.0 * s;
+    const double a_lo = fma((2.0 * s) * s2, q, 2.0 * s_lo);
+    // ln x = L_hi + L_lo (two-sum of e ln2_hi, exact, and a_hi)
+    const double E = (double)e;
+    const double p = E * kLn2Hi;
+    const double L_hi = p + a_hi;
+    const double bb = L_hi - p;
+    const double L_lo = ((p - (L_hi - bb)) + (a_hi - bb)) + fma(E, kLn2Lo, a_lo);
+    // y = t ln x = y_hi + y_lo
+    const double td = (double)t;
+    const double y_hi = td * L_hi;
+    if (!(fabs(y_hi) <= 700.0)) return (float)pow((double)x, (double)t);
+    const double y_lo = fma(td, L_hi, -y_hi) + td * L_lo;
+    const double n = rint(y_hi * kInvLn2);
+    const double r = fma(-n, kLn2Hi, y_hi) + fma(-n, kLn2Lo, y_lo);
+    double c = 1.0 / 6227020800.0;                          // 1/13!
+    c = fma(c, r, 1.0 / 479001600.0);
+    c = fma(c, r, 1.0 / 39916800.0);
+    c = fma(c, r, 1.0 / 3628800.0);
+    c = fma(c, r, 1.0 / 362880.0);
+    c = fma(c, r, 1.0 / 40320.0);
+    c = fma(c, r, 1.0 / 5040.0);
+    c = fma(c, r, 1.0 / 720.0);
+    c = fma(c, r, 1.0 / 120.0);
+    c = fma(c, r, 1.0 / 24.0);
+    c = fma(c, r, 1.0 / 6.0);
+    c = fma(c, r, 0.5);
+    const double er = 1.0 + fma(r * r, c, r);               // exp(r)
+    const double scale = u2d((uint64_t)((int)n + 1023) << 52);
+    return (float)(er * scale);
+}
+
+// x ** (float)(1/3) rounded to float (friction.py:66): the double power
+// rounded once.  PyTorch's CPU pow agrees with this value on all but a
 // small fraction of inputs, where it differs by one ulp.
 SWE_HD float pow_third(float x, float third) {
+#if defined(__CUDA_ARCH__)
+    return pow_pos(x, third);
+#else
     return (float)pow((double)x, (double)third);
+#endif
 }
 
 // Semi-implicit friction factor shared by both friction models

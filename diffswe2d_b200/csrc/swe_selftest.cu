@@ -11,7 +11,10 @@
 //              (a = b * m for m half-way between two floats, then its
 //              float neighbours), the cases a one-step correction can miss;
 //   which = 3: sqrt_cr(x) == __fsqrt_rn(x) for every float x in
-//              [2^-100, 2^100).
+//              [2^-100, 2^100);
+//   which = 4: pow_pos(x, t) == (float)pow((double)x, (double)t) for every
+//              float x in [2^-40, 2^14), t the float whose bit pattern is
+//              the low 32 bits of `seed`.
 // It returns the number of mismatches and the first mismatching input.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -72,6 +75,17 @@ __global__ void sqrt_exhaustive(unsigned long long* count, uint32_t* first) {
     }
 }
 
+__global__ void pow_exhaustive(unsigned long long* count, uint32_t* first, float t) {
+    const uint64_t n = (uint64_t)54 << 23;  // exponents -40..13, all significands
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t bits = (uint32_t)i + (87u << 23);
+        const float x = u2f(bits);
+        const float p = pow_pos(x, t);
+        if (f2u(p) != f2u((float)pow((double)x, (double)t))) record(count, first, bits, f2u(p));
+    }
+}
+
 __global__ void div_random(unsigned long long* count, uint32_t* first, uint64_t n, uint64_t seed) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
          t += (uint64_t)gridDim.x * blockDim.x) {
@@ -107,13 +121,14 @@ using namespace swe;
 // mismatching inputs); both are written by the call.
 extern "C" int swe_selftest_arith_f32(int which, long long n, unsigned long long seed,
                                       unsigned long long* count, uint32_t* first, void* stream) {
-    if (!count || !first || which < 0 || which > 3 || n < 0) return SWE_EARG;
+    if (!count || !first || which < 0 || which > 4 || n < 0) return SWE_EARG;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(count, 0, sizeof(unsigned long long), s) != cudaSuccess) return SWE_ECUDA;
     if (cudaMemsetAsync(first, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
     const int blocks = 148 * 8, threads = 256;
     if (which == 0) rcp_exhaustive<<<blocks, threads, 0, s>>>(count, first);
     else if (which == 3) sqrt_exhaustive<<<blocks, threads, 0, s>>>(count, first);
+    else if (which == 4) pow_exhaustive<<<blocks, threads, 0, s>>>(count, first, u2f((uint32_t)seed));
     else if (which == 1) div_random<<<blocks, threads, 0, s>>>(count, first, (uint64_t)n, seed);
     else div_midpoints<<<blocks, threads, 0, s>>>(count, first, (uint64_t)n, seed);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;

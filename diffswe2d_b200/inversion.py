@@ -172,7 +172,7 @@ def invert(problem: InversionProblem, raw0: torch.Tensor, lr: float = 0.002, max
         mse = ((sim - problem.targets) ** 2).mean(dim=(1, 2))
         rmse = mse.detach().sqrt().cpu().tolist()
         history.append(rmse)
-        losses.append(float(mse.sum()))
+        losses.append(float(mse.sum().detach()))
         for b in range(B):
             if reached[b] is None and rmse[b] <= rmse_tol:
                 reached[b] = it

@@ -7,6 +7,7 @@ square root are checked exhaustively over the range the step uses; the
 corrected division on random operands and on operands built next to rounding
 midpoints.
 """
+import numpy as np
 import pytest
 import torch
 
@@ -47,3 +48,23 @@ def test_division_random_operands(seed):
 def test_division_near_midpoints():
     bad, first = _selftest(2, n=1 << 30, seed=7)
     assert bad == 0, f"{bad} division mismatches, first (a, b) = {first}"
+
+
+
+def _f32_bits(v):
+    return int(np.array(v, dtype=np.float32).view(np.uint32))
+
+
+def test_friction_power_exhaustive():
+    """pow_pos, the friction's h ** (1/3), against CUDA's double pow rounded
+    to float, for every float h in [2^-40, 2^14)."""
+    bad, first = _selftest(4, seed=_f32_bits(np.float32(1.0 / 3.0)))
+    assert bad == 0, f"{bad} power mismatches, first (x, got) = {first}"
+
+
+def test_friction_power_derivative_exponent():
+    """The adjoint's h ** (1/3 - 1) (exponent rounded to float as the
+    kernel rounds it): at most a handful of near-midpoint cases may round
+    the other way, a one-ulp difference in a derivative."""
+    bad, first = _selftest(4, seed=_f32_bits(np.float32(1.0 / 3.0) - np.float32(1.0)))
+    assert bad <= 8, f"{bad} power mismatches, first (x, got) = {first}"
