@@ -55,8 +55,9 @@ struct SweConsts {
 // the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The
 // device self-test swe_selftest_arith_f32 checks rcp_cr against CUDA's
 // rcp.rn for every float in the range used and div_by against div.rn on
-// random and near-halfway operands.  Quotients outside [2^-100, 2^100]
-// (zero excepted) and non-finite operands take the IEEE division instead.
+// random and near-halfway operands, and on tiny numerators.  Quotients
+// outside [2^-100, 2^100] or below 2^-125 (zero excepted) and non-finite
+// operands take the IEEE division instead.
 #if defined(__CUDA_ARCH__)
 // IEEE fallbacks for operands outside the range the fast forms are checked
 // for.  Out of line: one copy shared by every call site keeps the kernels'
@@ -79,15 +80,22 @@ SWE_HD float rcp_cr(float b) {
 #endif
 }
 
-// a / b given y = rcp_cr(b).
+// a / b given y = rcp_cr(b).  The FMA remainder r = a - q b must not
+// underflow, so a numerator below 2^-62 in magnitude (tiny and subnormal
+// momenta are common where thin films drain under friction) is scaled by
+// 2^64 first, exactly, and the quotient scaled back by 2^-64, exactly while
+// it stays at least 2^-126: the range test on the scaled quotient (at least
+// 2^-61) ensures that.  Subnormal quotients take the IEEE division.
 SWE_HD float div_by(float a, float b, float y) {
 #if defined(__CUDA_ARCH__)
-    const float q = __fmul_rn(a, y);
-    const float r = __fmaf_rn(-q, b, a);
+    const bool tiny = fabsf(a) < 0x1p-62f;
+    const float as = tiny ? __fmul_rn(a, 0x1p+64f) : a;
+    const float q = __fmul_rn(as, y);
+    const float r = __fmaf_rn(-q, b, as);
     const float q1 = __fmaf_rn(r, y, q);
     const float aq = fabsf(q);
-    const bool safe = (aq >= 0x1p-100f && aq <= 0x1p+100f) || a == 0.0f;
-    return safe ? q1 : ieee_div_slow(a, b);
+    const bool safe = (aq >= (tiny ? 0x1p-61f : 0x1p-100f) && aq <= 0x1p+100f) || a == 0.0f;
+    return safe ? (tiny ? __fmul_rn(q1, 0x1p-64f) : q1) : ieee_div_slow(a, b);
 #else
     (void)y;
     return a / b;

@@ -14,7 +14,11 @@
 //              [2^-100, 2^100);
 //   which = 4: pow_pos(x, t) == (float)pow((double)x, (double)t) for every
 //              float x in [2^-40, 2^14), t the float whose bit pattern is
-//              the low 32 bits of `seed`.
+//              the low 32 bits of `seed`;
+//   which = 5: div_by(a, b, rcp_cr(b)) == __fdiv_rn(a, b) for n draws of b
+//              in [2^-20, 2^20) and six tiny numerators each: one random
+//              below 2^-62 (subnormals included) and five next to a
+//              quotient midpoint, scaled by 2^-90.
 // It returns the number of mismatches and the first mismatching input.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -86,6 +90,27 @@ __global__ void pow_exhaustive(unsigned long long* count, uint32_t* first, float
     }
 }
 
+__global__ void div_tiny(unsigned long long* count, uint32_t* first, uint64_t n, uint64_t seed) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const float b = rand_float(seed ^ (t * 3 + 0x2468aceull), -20, 19);
+        float as[6];
+        // random: exponent field 0..64 (subnormals and [2^-126, 2^-62))
+        const uint32_t h = hash32(seed ^ (t * 3 + 1 + 0x1f2e3dull));
+        const uint32_t ef = hash32(seed ^ (t * 3 + 2 + 0x5a5a5aull)) % 65u;
+        as[0] = u2f((ef << 23) | (h & 0x7fffffu) | ((h >> 31) << 31));
+        // next to a midpoint of the quotient, scaled down by 2^-90
+        const float m0 = rand_float(seed ^ (t * 3 + 0xabcdefull), -10, 10);
+        const double mid = 0.5 * ((double)m0 + (double)u2f(f2u(m0) + 1u));
+        const float a0 = (float)((double)b * mid * 0x1p-90);
+        for (int d = -2; d <= 2; ++d) as[3 + d] = u2f(f2u(a0) + (uint32_t)d);
+        for (int k = 0; k < 6; ++k) {
+            const float q = div_by(as[k], b, rcp_cr(b));
+            if (f2u(q) != f2u(__fdiv_rn(as[k], b))) record(count, first, f2u(as[k]), f2u(b));
+        }
+    }
+}
+
 __global__ void div_random(unsigned long long* count, uint32_t* first, uint64_t n, uint64_t seed) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
          t += (uint64_t)gridDim.x * blockDim.x) {
@@ -121,7 +146,7 @@ using namespace swe;
 // mismatching inputs); both are written by the call.
 extern "C" int swe_selftest_arith_f32(int which, long long n, unsigned long long seed,
                                       unsigned long long* count, uint32_t* first, void* stream) {
-    if (!count || !first || which < 0 || which > 4 || n < 0) return SWE_EARG;
+    if (!count || !first || which < 0 || which > 5 || n < 0) return SWE_EARG;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(count, 0, sizeof(unsigned long long), s) != cudaSuccess) return SWE_ECUDA;
     if (cudaMemsetAsync(first, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
@@ -129,6 +154,7 @@ extern "C" int swe_selftest_arith_f32(int which, long long n, unsigned long long
     if (which == 0) rcp_exhaustive<<<blocks, threads, 0, s>>>(count, first);
     else if (which == 3) sqrt_exhaustive<<<blocks, threads, 0, s>>>(count, first);
     else if (which == 4) pow_exhaustive<<<blocks, threads, 0, s>>>(count, first, u2f((uint32_t)seed));
+    else if (which == 5) div_tiny<<<blocks, threads, 0, s>>>(count, first, (uint64_t)n, seed);
     else if (which == 1) div_random<<<blocks, threads, 0, s>>>(count, first, (uint64_t)n, seed);
     else div_midpoints<<<blocks, threads, 0, s>>>(count, first, (uint64_t)n, seed);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;

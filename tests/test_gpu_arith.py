@@ -68,3 +68,11 @@ def test_friction_power_derivative_exponent():
     the other way, a one-ulp difference in a derivative."""
     bad, first = _selftest(4, seed=_f32_bits(np.float32(1.0 / 3.0) - np.float32(1.0)))
     assert bad <= 8, f"{bad} power mismatches, first (x, got) = {first}"
+
+
+def test_division_tiny_numerators():
+    """The shared-reciprocal quotient on numerators below 2^-62, subnormals
+    included, which it scales by 2^64 (subnormal quotients take the IEEE
+    division): it equals IEEE division."""
+    bad, first = _selftest(5, n=1 << 28, seed=3)
+    assert bad == 0, f"{bad} division mismatches, first (a, b) = {first}"

@@ -102,6 +102,36 @@ def test_odd_and_tile_straddling_sizes(shape):
         assert dt == dto
 
 
+
+def test_tiny_and_subnormal_operands():
+    """Cells whose momenta are tiny or subnormal make quotients leave the
+    range of the kernels' fast division (the sweep then recomputes its tile
+    with the exact IEEE fallbacks); the result must still equal the oracle
+    bit for bit."""
+    rng = np.random.default_rng(11)
+    B, ny, nx = 1, 96, 160
+    h = rng.uniform(0.05, 0.5, (B, ny, nx))
+    hu = rng.normal(0, 0.05, h.shape)
+    hv = rng.normal(0, 0.05, h.shape)
+    pick = rng.uniform(size=h.shape)
+    hu[pick < 0.05] = 1e-36
+    hv[(pick >= 0.05) & (pick < 0.08)] = -3e-39  # subnormal in float32
+    h[(pick >= 0.08) & (pick < 0.10)] = 1e-30    # below the dry depth
+    U = np.stack([h, hu, hv], axis=1).astype(np.float32)
+    assert (np.abs(U[:, 2]) < np.finfo(np.float32).tiny).any()
+    bed = rng.normal(-0.2, 0.05, (1, 1, ny, nx)).astype(np.float32)
+    n = np.full_like(bed, 0.03)
+    cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                    boundary_bottom="wall", constant_level=0.05)
+    m = _model(bed[0, 0], n[0, 0], 0.05, 0.05, cfg)
+    om = OracleSWE(bed, n, 0.05, 0.05, cfg)
+    Ug, Uo = _t(U), U
+    for k in range(3):
+        Ug, dt = m.step(Ug, 0.0, 0.01)
+        Uo, dto = om.step(Uo, 0.0, 0.01)
+        assert np.array_equal(_np(Ug).view(np.uint32), Uo.view(np.uint32)), f"step {k + 1}"
+        assert dt == dto
+
 def _run(m, U, nsteps, dynamic=False):
     t = 0.0
     dts = []
