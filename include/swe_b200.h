@@ -487,15 +487,21 @@ int swe_friction_f32(const float* U, const float* n, int nB, int B, int ny, int 
                      int model, const swe_params* p, float* out, void* stream);
 
 /*
- * Device self-test of the step's division and square root (no counterpart
- * in the reference; it checks that the step's arithmetic is the IEEE
- * correctly-rounded arithmetic of the reference's float32 tensors).
+ * Device self-test of the step's division, square root and friction power
+ * (no counterpart in the reference; it checks that the step's arithmetic is
+ * the IEEE correctly-rounded arithmetic of the reference's float32 tensors).
  * which = 0: reciprocal, exhaustive over |b| in [2^-100, 2^100);
  * which = 1: division on n random operand pairs (seed);
  * which = 2: division on n operand pairs built next to rounding midpoints;
- * which = 3: square root, exhaustive over [2^-100, 2^100).
+ * which = 3: square root, exhaustive over [2^-100, 2^100);
+ * which = 4: x ** t (t = the float with the bit pattern seed & 0xffffffff)
+ *            against the double pow rounded to float, every x in
+ *            [2^-40, 2^14);
+ * which = 5: division with numerators below 2^-62 (subnormals included) on
+ *            n draws of six operand pairs.
  * count (device, 1 x u64) receives the number of mismatches against CUDA's
- * rcp.rn / div.rn / sqrt.rn, first (device, 2 x u32) the first bad input.
+ * rcp.rn / div.rn / sqrt.rn / pow, first (device, 2 x u32) the first bad
+ * input.
  */
 int swe_selftest_arith_f32(int which, long long n, unsigned long long seed,
                            unsigned long long* count, uint32_t* first, void* stream);
