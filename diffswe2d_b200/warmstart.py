@@ -4,7 +4,7 @@ A 1D-conv encoder plus MLP maps the gauge waveforms of a run (6 gauges x
 1125 samples, eta every 0.02 s over 22.5 s) to the 16 spline controls of the
 west-edge inflow.  Its prediction seeds the adjoint inversion
 (``inversion.invert``); the plain inversion from the reference's cold start
-stays the fallback and the judge of the error (the reference has no learned
+stays the fallback and the measure of the error (the reference has no learned
 part; its inversion is
 ``Examples/inverse/Monai_Valley/Monai_Velley_BC_inversion_spline_lr002/
 bc_inversion_train.py:648-768``).

@@ -1,7 +1,7 @@
 """The hand-written adjoint against the reference's autograd gradients and
 against finite differences of the FP64 oracle.
 
-Bar (north_star): adjoint gradients match the reference autograd to 1e-4
+Bar: adjoint gradients match the reference autograd to 1e-4
 (normwise relative, per gradient).  Fixtures: tests/golden/adj_*.npz, made by
 the reference itself (make_golden_adjoint.py) in float32 with
 correctly-rounded sqrt/pow and in float64.
