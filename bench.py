@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--arithmetic", choices=["exact", "fast"], default="exact")
     ap.add_argument("--ny", type=int, default=4096)
     ap.add_argument("--nx", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -468,15 +469,15 @@ def main():
     cfg = SWEConfig(**sc.config)
     # launch shape from the project's autotuner (sweep tile rows per size class)
     from diffswe2d_b200 import autotune
-    tuning = autotune.tune(dev)
-    autotune.apply(dev, cells)
-    rows_used = autotune.tuned_rows(cells, dev)
+    tuning = autotune.tune(dev, arithmetic=args.arithmetic)
+    autotune.apply(dev, cells, args.arithmetic)
+    rows_used = autotune.tuned_rows(cells, dev, args.arithmetic)
     model = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev),
-                  sc.dx, sc.dy, config=cfg, train_dem=False)
+                  sc.dx, sc.dy, config=cfg, train_dem=False, arithmetic=args.arithmetic)
     model.set_dynamic_boundary(torch.from_numpy(sc.bc_times).to(dev),
                                torch.from_numpy(sc.bc_levels).to(dev))
     lib = nat.lib()
-    p = nat.params(cfg, sc.dx, sc.dy)
+    p = nat.params(cfg, sc.dx, sc.dy, args.arithmetic)
     bed = model.bed.detach().contiguous()
     n = model.roughness_length.contiguous()
     U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]

@@ -6,6 +6,7 @@ kernels behind the C ABI of ``include/swe_b200.h``.
 """
 from .boundary import add_ghost_cells
 from .config import SWEConfig
+from .forcing import RainfallForcing
 from .friction import apply_manning_friction, apply_roughness_length_friction
 from .numerics import limited_increment, minmod3
 from .reconstruction import bflood_cn_reconstruction
@@ -15,6 +16,7 @@ from .solver import SWE2D
 __all__ = [
     "SWEConfig",
     "SWE2D",
+    "RainfallForcing",
     "add_ghost_cells",
     "bflood_cn_reconstruction",
     "bflood_hllc_flux",

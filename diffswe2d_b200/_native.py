@@ -14,6 +14,10 @@ import torch
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libswe_b200.so"
 
 SWE_OK, SWE_EARG, SWE_ECUDA = 0, 1, 2
+#: swe_params.arithmetic: IEEE operation-for-operation kernels, or the
+#: tolerance-mode kernels
+ARITH_EXACT, ARITH_FAST = 0, 1
+ARITHMETIC = {"exact": ARITH_EXACT, "fast": ARITH_FAST}
 S_NONFINITE_STATE, S_NONFINITE_DT, S_NONPOSITIVE_DT, S_STEP_LIMIT = 1, 2, 4, 8
 RED_WORDS = 8
 FORCING_NONE, FORCING_SCALAR, FORCING_FIELD = 0, 1, 2
@@ -50,6 +54,8 @@ class SweParams(ctypes.Structure):
         ("positivity_limiter", ctypes.c_int32),
         ("apply_friction", ctypes.c_int32),
         ("friction_model", ctypes.c_int32),
+        ("arithmetic", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -140,6 +146,8 @@ _SIGNATURES = {
                      _P, _I, _I, _P, _P, _P, _P],
     "swe_step_stage_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                            _F, _P, _I, _I, _P, _P, _P, _P],
+    "swe_step_stage_forced_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P,
+                                  _I, _F, _P, _I, _I, _P, _I, _I, _P, _P, _P, _P],
     "swe_clock_f32": [_P, _P, _P, _P, _I, _P, _P, _I, _I, _P, _I, _P, _I, _P],
     "swe_run_clock_f32": [_P, _P, _P, _I, _P, _P, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _P],
     "swe_gauge_adjoint_f32": [_P, _I, _I, _I, _P, _I, _P, _I, _I, _P],
@@ -171,7 +179,7 @@ _SIGNATURES = {
     "swe_selftest_arith_f32": [_I, ctypes.c_longlong, ctypes.c_ulonglong, _P, _P, _P],
     "swe_ensemble_prepare_f32": [ctypes.POINTER(SweEnsembleMember), _I, _P, _P],
     "swe_ensemble_reset_f32": [_P, _I, _P],
-    "swe_ensemble_run_f32": [_P, _I, _I, _I, _P],
+    "swe_ensemble_run_f32": [_P, _I, _I, _I, _I, ctypes.c_longlong, _P],
     "swe_ensemble_results_f32": [_P, _I, _P, _P, _P],
     "swe_tune_sweep_rows": [_I],
     "swe_sweep_rows": [],
@@ -225,7 +233,13 @@ def exported_symbols():
     return list(_SIGNATURES)
 
 
-def params(cfg, dx: float, dy: float) -> SweParams:
+def arithmetic_code(arithmetic: str) -> int:
+    if arithmetic not in ARITHMETIC:
+        raise ValueError(f"arithmetic must be one of {sorted(ARITHMETIC)}, got {arithmetic!r}")
+    return ARITHMETIC[arithmetic]
+
+
+def params(cfg, dx: float, dy: float, arithmetic: str = "exact") -> SweParams:
     for side in ("left", "right", "top", "bottom"):
         name = getattr(cfg, f"boundary_{side}")
         if name not in BC_CODES:
@@ -240,6 +254,7 @@ def params(cfg, dx: float, dy: float) -> SweParams:
         BC_CODES[cfg.boundary_top], BC_CODES[cfg.boundary_bottom],
         int(bool(cfg.water_slope_reset)), int(bool(cfg.positivity_limiter)),
         int(bool(cfg.apply_friction)), 0 if cfg.frictionmodel == "manning" else 1,
+        arithmetic_code(arithmetic), 0,
     )
 
 
@@ -277,4 +292,4 @@ def params_basic(gravity=9.81, epsilon=1e-12, dry_depth=1e-6, theta=1.3,
     l, r, t, b = bcs if bcs is not None else ("transmissive",) * 4
     return SweParams(float(gravity), float(dry_depth), float(epsilon), 0.5, float(theta), 1.0, 1.0,
                      float(constant_value), BC_CODES[l], BC_CODES[r], BC_CODES[t], BC_CODES[b],
-                     int(bool(water_slope_reset)), int(bool(positivity_limiter)), 1, 0)
+                     int(bool(water_slope_reset)), int(bool(positivity_limiter)), 1, 0, ARITH_EXACT, 0)

@@ -13,6 +13,8 @@ Two knobs are tuned by timing them on the GPU in use:
   loop -- more steps per replay mean fewer host reads, more no-op steps at
   the end of a call.
 
+Tile heights are tuned separately for the two arithmetic modes of the step
+kernels ("exact" and "fast"), whose register use and cost per cell differ.
 Results are kept per device name in memory and in
 ``$XDG_CACHE_HOME/diffswe2d_b200/autotune.json`` (default ``~/.cache``).
 """
@@ -76,14 +78,20 @@ def size_class(cells: int) -> int:
     return len(SIZE_CLASSES) - 1
 
 
-def tuned_rows(cells: int, device="cuda") -> int:
+def _mode_key(name: str, arithmetic: str) -> str:
+    nat.arithmetic_code(arithmetic)
+    return name if arithmetic == "exact" else f"{name}_{arithmetic}"
+
+
+def tuned_rows(cells: int, device="cuda", arithmetic: str = "exact") -> int:
     """Tile height for a grid of `cells` cells (the default if not tuned)."""
     k = size_class(cells)
-    rows = _load(device).get("rows")
+    rows = _load(device).get(_mode_key("rows", arithmetic))
     return int(rows[k]) if rows else DEFAULT_ROWS[k]
 
 
-def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int, batch: int = 1) -> float:
+def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int, batch: int = 1,
+                arithmetic: str = "exact") -> float:
     """ms per step of the single-grid step kernels on a runup-recipe grid
     (``batch`` copies of it)."""
     from . import scenarios
@@ -91,7 +99,7 @@ def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int, batch: 
     sc = scenarios.tiled(scenarios.runup(seed=0), side_y, side_x)
     dev = torch.device(device)
     lib = nat.lib()
-    p = nat.params(SWEConfig(**sc.config), sc.dx, sc.dy)
+    p = nat.params(SWEConfig(**sc.config), sc.dx, sc.dy, arithmetic)
     bed = torch.from_numpy(sc.bed).to(dev)
     n = torch.from_numpy(sc.roughness).to(dev)
     U0 = torch.from_numpy(sc.U0).to(dev).expand(batch, 3, side_y, side_x).contiguous()
@@ -118,11 +126,13 @@ def _time_steps(side_y: int, side_x: int, rows: int, device, steps: int, batch: 
     return e0.elapsed_time(e1) / steps
 
 
-def tune(device="cuda", steps: int = 8, force: bool = False) -> dict:
-    """Time every tile height on one representative grid per size class and
-    the graph chunk length on a small grid; store and return the choice."""
+def tune(device="cuda", steps: int = 8, force: bool = False, arithmetic: str = "exact") -> dict:
+    """Time every tile height on one representative grid per size class
+    (kernels of the given arithmetic), the ensemble tile height and the
+    graph chunk length on a small grid; store and return the choice."""
     entry = dict(_load(device))
-    if entry.get("rows") and not force:
+    rkey = _mode_key("rows", arithmetic)
+    if entry.get(rkey) and not force:
         return entry
     t0 = time.perf_counter()
     reps = ((96, 160), (384, 512), (1024, 960), (2048, 2048))
@@ -130,17 +140,18 @@ def tune(device="cuda", steps: int = 8, force: bool = False) -> dict:
     for k, (ny, nx) in enumerate(reps):
         best, best_ms = None, None
         for r in ROW_CHOICES:
-            ms = _time_steps(ny, nx, r, device, steps)
+            ms = _time_steps(ny, nx, r, device, steps, arithmetic=arithmetic)
             timing[f"{ny}x{nx}/rows{r}"] = ms
             if best_ms is None or ms < best_ms:
                 best, best_ms = r, ms
         rows_choice.append(best)
     nat.check(nat.lib().swe_tune_sweep_rows(64), "tune rows")
-    entry["rows"] = rows_choice
-    entry["chunk"] = _tune_chunk(device)
-    entry["ensemble_rows"] = _tune_ensemble_rows(device)
-    entry["timing_ms"] = timing
-    entry["seconds"] = time.perf_counter() - t0
+    entry[rkey] = rows_choice
+    if not entry.get("chunk") or force:
+        entry["chunk"] = _tune_chunk(device)
+    entry[_mode_key("ensemble_rows", arithmetic)] = _tune_ensemble_rows(device, arithmetic=arithmetic)
+    entry[_mode_key("timing_ms", arithmetic)] = timing
+    entry[_mode_key("seconds", arithmetic)] = time.perf_counter() - t0
     _store(device, entry)
     return entry
 
@@ -148,7 +159,7 @@ def tune(device="cuda", steps: int = 8, force: bool = False) -> dict:
 ENSEMBLE_ROW_CHOICES = (8, 16, 32, 64)
 
 
-def _tune_ensemble_rows(device, count: int = 24, steps: int = 30) -> int:
+def _tune_ensemble_rows(device, count: int = 24, steps: int = 30, arithmetic: str = "exact") -> int:
     """Tile height for the persistent ensemble kernel, where many scenarios
     fill the GPU together (throughput, not per-step latency, decides): one
     value for all scenarios, timed on `count` seeded scenarios with sides
@@ -163,7 +174,7 @@ def _tune_ensemble_rows(device, count: int = 24, steps: int = 30) -> int:
         members.append(sc)
     best, best_ms = None, None
     for r in ENSEMBLE_ROW_CHOICES:
-        ens = Ensemble(members, device=device, rows=r)
+        ens = Ensemble(members, device=device, rows=r, arithmetic=arithmetic)
         ens.run()
         ms = ens.run().elapsed_ms
         if best_ms is None or ms < best_ms:
@@ -172,9 +183,9 @@ def _tune_ensemble_rows(device, count: int = 24, steps: int = 30) -> int:
     return int(best)
 
 
-def tuned_ensemble_rows(device="cuda") -> int:
+def tuned_ensemble_rows(device="cuda", arithmetic: str = "exact") -> int:
     """The ensemble kernel's tile height (16 if not tuned)."""
-    return int(_load(device).get("ensemble_rows", 16))
+    return int(_load(device).get(_mode_key("ensemble_rows", arithmetic), 16))
 
 
 def _tune_chunk(device) -> int:
@@ -201,11 +212,12 @@ def _tune_chunk(device) -> int:
     return int(best)
 
 
-def tuned_rows_for_shape(batch: int, ny: int, nx: int, device="cuda", steps: int = 6) -> int:
+def tuned_rows_for_shape(batch: int, ny: int, nx: int, device="cuda", steps: int = 6,
+                         arithmetic: str = "exact") -> int:
     """Tile height for a time loop over [batch, 3, ny, nx] states: timed on
     that shape (runup recipe) the first time it is asked for, then cached."""
     entry = _load(device)
-    key = f"{batch}x{ny}x{nx}"
+    key = f"{batch}x{ny}x{nx}" if arithmetic == "exact" else f"{arithmetic}/{batch}x{ny}x{nx}"
     shapes = entry.setdefault("shapes", {})
     if key in shapes:
         return int(shapes[key])
@@ -215,7 +227,7 @@ def tuned_rows_for_shape(batch: int, ny: int, nx: int, device="cuda", steps: int
         for r in ROW_CHOICES:
             if r > 2 * ny and best is not None:
                 break
-            ms = _time_steps(ny, nx, r, device, steps, batch)
+            ms = _time_steps(ny, nx, r, device, steps, batch, arithmetic)
             if best_ms is None or ms < best_ms:
                 best, best_ms = r, ms
     finally:
@@ -242,12 +254,12 @@ class sweep_rows:
         return False
 
 
-def apply(device="cuda", cells: Optional[int] = None) -> None:
+def apply(device="cuda", cells: Optional[int] = None, arithmetic: str = "exact") -> None:
     """Use the tuned values: tile height for grids of `cells` cells (single-grid
-    kernels) and the forward() chunk length."""
+    kernels of the given arithmetic) and the forward() chunk length."""
     entry = _load(device)
     if cells is not None:
-        nat.check(nat.lib().swe_tune_sweep_rows(tuned_rows(cells, device)), "tune rows")
+        nat.check(nat.lib().swe_tune_sweep_rows(tuned_rows(cells, device, arithmetic)), "tune rows")
     if entry.get("chunk"):
         from .solver import SWE2D
         SWE2D.steps_per_chunk = int(entry["chunk"])

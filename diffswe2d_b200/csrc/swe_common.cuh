@@ -66,7 +66,8 @@ inline bool valid_params(const swe_params* p) {
     if (!(p->gravity > 0.0) || !(p->epsilon > 0.0) || !(p->dry_depth >= 0.0)) return false;
     if (!(p->dx > 0.0) || !(p->dy > 0.0)) return false;
     return valid_bc(p->bc_left) && valid_bc(p->bc_right) && valid_bc(p->bc_top) &&
-           valid_bc(p->bc_bottom) && (p->friction_model == 0 || p->friction_model == 1);
+           valid_bc(p->bc_bottom) && (p->friction_model == 0 || p->friction_model == 1) &&
+           (p->arithmetic == SWE_ARITH_EXACT || p->arithmetic == SWE_ARITH_FAST);
 }
 
 }  // namespace swe

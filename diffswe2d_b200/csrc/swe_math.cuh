@@ -606,8 +606,15 @@ SWE_HD State roughness_friction(State s, float z0, float dt, const SweConsts& k)
 // stable dt, solver.py:620-626: cfl / clamp(ax/dx + ay/dy, min=eps), where
 // PyTorch evaluates `scalar / tensor` as tensor.reciprocal() * scalar.
 SWE_HD float stable_dt(float ax, float ay, const SweConsts& k) {
+#if defined(__CUDA_ARCH__)
+    // IEEE divisions whatever the file's division flags (the tolerance-mode
+    // kernels are compiled with approximate "/").
+    float den = fmaxf(__fadd_rn(__fdiv_rn(ax, k.dx), __fdiv_rn(ay, k.dy)), k.eps);
+    return __fmul_rn(__frcp_rn(den), k.cfl);
+#else
     float den = fmaxf(ax / k.dx + ay / k.dy, k.eps);
     return (1.0f / den) * k.cfl;
+#endif
 }
 
 }  // namespace swe

@@ -27,6 +27,8 @@
 #include <string.h>
 
 #include "swe_common.cuh"
+#include "swe_sweep.cuh"
+#include "swe_ensemble.cuh"
 
 namespace swe {
 namespace {
@@ -38,40 +40,6 @@ constexpr int NYS = (TY + 2) * TX;  // y-direction side cells per tile
 constexpr int NXF = TY * (TX + 1);  // x faces per tile
 constexpr int NYF = (TY + 1) * TX;  // y faces per tile
 
-struct StepArgs {
-    const float* U;
-    const float* bed;
-    const float* n;
-    const float* level;
-    const float* rain;
-    const float* infil;
-    float* tend;   // stage 1: k1 output; stage 2: k1 input
-    float* U_out;  // stage 2 output
-    uint32_t* red;
-    const swe_clock* clk;  // device clock of forward(), or null for a plain step
-    float* hmax;           // running max depth [B,ny,nx], or null
-    int rows;              // output rows per sweep tile
-    float max_dt, cval;
-    int B, bedB, nB, levelB, ny, nx;
-    int rain_mode, rain_batch, infil_mode, infil_batch;
-    int bc[4];
-    int wsr, positivity, friction, friction_model;
-    SweConsts kc;
-};
-
-__device__ __forceinline__ size_t at3(int b, int c, int j, int i, int ny, int nx) {
-    return (((size_t)b * 3 + c) * ny + j) * nx + i;
-}
-__device__ __forceinline__ size_t at1(int b, int j, int i, int ny, int nx) {
-    return ((size_t)b * ny + j) * nx + i;
-}
-
-__device__ __forceinline__ float forcing(const float* f, int mode, int fb, int b, int j, int i,
-                                         int ny, int nx) {
-    if (mode == SWE_FORCING_SCALAR) return f[0];
-    if (mode == SWE_FORCING_FIELD) return f[at1(fb == 1 ? 0 : b, j, i, ny, nx)];
-    return 0.0f;
-}
 
 // State of interior cell (j, i) as the stage sees it: U for stage 1, the
 // predictor clean(U, U + hdt*k1) (solver.py:639) for stage 2.
@@ -85,9 +53,6 @@ __device__ __forceinline__ State interior_state(const StepArgs& a, int b, int j,
     return clean_and_limit(u, c, a.kc, a.positivity != 0);
 }
 
-__device__ __forceinline__ float bed_at(const StepArgs& a, int b, int j, int i) {
-    return a.bed[at1(a.bedB == 1 ? 0 : b, j, i, a.ny, a.nx)];
-}
 
 // Padded cell (j, i) (interior coordinates, -2 <= j < ny+2) with the ghost
 // rules of add_ghost_cells.  Only the four "arms" of the padding are ever
@@ -156,8 +121,6 @@ __device__ __forceinline__ void region_cell(const StepArgs& a, int b, int j, int
         else s.hv = val;
     }
 }
-
-__device__ __forceinline__ uint32_t warp_max_u32(uint32_t v) { return __reduce_max_sync(0xffffffffu, v); }
 
 template <int STAGE>
 __global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
@@ -310,6 +273,16 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
     }
 }
 
+// Stage-2 predictor of the IEEE kernels: clean(U, U + hdt*k1) in the
+// reference's operation order (solver.py:639).
+struct ExactPredict {
+    static __device__ __forceinline__ State predict(const State& u, float k0, float k1, float k2,
+                                                    float hdt, const SweConsts& k, int positivity) {
+        const State c{u.h + hdt * k0, u.hu + hdt * k1, u.hv + hdt * k2};
+        return clean_and_limit(u, c, k, positivity != 0);
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Row-sweep form of the two stages.
 //
@@ -321,98 +294,6 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StepArgs a) {
 // the warp computes one primitive, one x-side, one y-side, one x-face and
 // one y-face (plus 4/28 of a column and 4/SW_ROWS of a row of halo), with no
 // shared memory and no block barrier.
-constexpr int SW_OUT = 28;    // output columns per warp
-constexpr int SW_ROWS = 64;   // output rows per warp
-constexpr int SW_WARPS = 4;   // warps per block (side by side in x)
-
-// Cell (j, i) of the padded state for the sweep, ghost rules as region_cell;
-// also returns the raw U of an interior cell (for stage 2's corrector).
-// Loads of the state and the tendency.  CG = true bypasses L1 (ld.global.cg):
-// needed when another block of the same launch wrote the data (the
-// persistent ensemble kernel), since L1 is not coherent across blocks.
-template <bool CG>
-__device__ __forceinline__ float ld_state(const float* p) {
-    return CG ? __ldcg(p) : *p;
-}
-
-// The second source cell of a wall ghost two cells out (rare: domain edge
-// only), kept out of line to keep the sweep kernels' code small.
-template <int STAGE, bool CG>
-__device__ __noinline__ State mirror_state(const float* __restrict__ U, const float* __restrict__ tend,
-                                           int ny, int nx, int b, int j, int i, float hdt, float eps,
-                                           float dry, int positivity) {
-    const size_t plane = (size_t)ny * nx;
-    const size_t o = at3(b, 0, j, i, ny, nx);
-    const State u{ld_state<CG>(U + o), ld_state<CG>(U + o + plane), ld_state<CG>(U + o + 2 * plane)};
-    if (STAGE == 1) return u;
-    const State c{u.h + hdt * ld_state<CG>(tend + o), u.hu + hdt * ld_state<CG>(tend + o + plane),
-                  u.hv + hdt * ld_state<CG>(tend + o + 2 * plane)};
-    SweConsts k{};
-    k.eps = eps;
-    k.dry = dry;
-    return clean_and_limit(u, c, k, positivity != 0);
-}
-
-template <int STAGE, bool CG>
-__device__ __forceinline__ void sweep_cell(const StepArgs& a, int b, int j, int i, float hdt,
-                                           State& s, float& z, State& uraw) {
-    const int ny = a.ny, nx = a.nx;
-    const bool jin = (unsigned)j < (unsigned)ny, iin = (unsigned)i < (unsigned)nx;
-    int js = min(max(j, 0), ny - 1), is = min(max(i, 0), nx - 1);
-    const bool xarm = jin && !iin && i >= -2 && i < nx + 2;
-    const bool yarm = iin && !jin && j >= -2 && j < ny + 2;
-    int code = -1, side = 0;
-    if (xarm || yarm) {
-        side = xarm ? (i < 0 ? 0 : 1) : (j < 0 ? 2 : 3);
-        code = a.bc[side];
-        if (code == SWE_BC_PERIODIC) {  // boundary.py:247-257, :301-302
-            if (xarm) is = i < 0 ? nx + i : i - nx;
-            else js = j < 0 ? ny + j : j - ny;
-        }
-    }
-    const size_t plane = (size_t)ny * nx;
-    const size_t o = at3(b, 0, js, is, ny, nx);
-    uraw = State{ld_state<CG>(a.U + o), ld_state<CG>(a.U + o + plane), ld_state<CG>(a.U + o + 2 * plane)};
-    if (STAGE == 1) {
-        s = uraw;
-    } else {  // predictor clean(U, U + dt/2 k1), solver.py:639
-        const State c{uraw.h + hdt * ld_state<CG>(a.tend + o), uraw.hu + hdt * ld_state<CG>(a.tend + o + plane),
-                      uraw.hv + hdt * ld_state<CG>(a.tend + o + 2 * plane)};
-        s = clean_and_limit(uraw, c, a.kc, a.positivity != 0);
-    }
-    z = bed_at(a, b, js, is);
-    if (code < 0 || code == SWE_BC_TRANSMISSIVE || code == SWE_BC_PERIODIC) return;
-    const float lev = ld_state<CG>(a.level + (a.levelB == 1 ? 0 : b));
-    if (code == SWE_BC_CONSTANT) {  // boundary.py:304-305
-        s = State{a.cval, a.cval, a.cval};
-    } else if (code == SWE_BC_WATER_LEVEL) {  // boundary.py:279-282, :307-310
-        s.h = fmaxf(lev - z, 0.0f);
-    } else if (code == SWE_BC_WALL) {  // boundary.py:312-316: flip of the first/last two lines
-        const int jm = xarm ? j : (j < 0 ? -1 - j : 2 * ny - 1 - j);
-        const int im = xarm ? (i < 0 ? -1 - i : 2 * nx - 1 - i) : i;
-        float mirror;
-        if (jm == js && im == is) {
-            mirror = xarm ? s.hu : s.hv;
-        } else {
-            const State m = mirror_state<STAGE, CG>(a.U, a.tend, ny, nx, b, jm, im, hdt, a.kc.eps,
-                                                    a.kc.dry, a.positivity);
-            mirror = xarm ? m.hu : m.hv;
-        }
-        if (xarm) s.hu = -mirror;
-        else s.hv = -mirror;
-    } else if (code == SWE_BC_ABSORBING) {  // boundary.py:318-328
-        const float hr = fmaxf(lev - z, 0.0f);
-        const float hg = s.h;
-        const float hc = hr > a.kc.absorb_lim ? hr : hg;
-        const float c = sqrtf(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
-        const float val = ((side == 0 || side == 2) ? -c : c) * (hg - hr);
-        if (xarm) s.hu = val;
-        else s.hv = val;
-    }
-}
-
-__device__ __forceinline__ float shfl_up1(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-__device__ __forceinline__ float shfl_dn1(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
 // FRIC: 0 no friction, 1 Manning, 2 roughness length (stage 2 only).
 // One tile of the sweep: SW_WARPS strips side by side (tile column bx) times
@@ -444,19 +325,8 @@ __device__ __forceinline__ void sweep_tile(const StepArgs& a, int bx, int by, in
 
     float dt = 0.0f, hdt = 0.0f;
     if (STAGE == 2) {
-        const uint32_t ax = CG ? __ldcg(a.red) : a.red[0];
-        const uint32_t ay = CG ? __ldcg(a.red + 1) : a.red[1];
-        const float st = stable_dt(u2f(ax), u2f(ay), kc);
-        const float max_dt = a.clk != nullptr ? a.clk->max_dt : a.max_dt;
-        dt = st != st ? st : fminf(st, max_dt);
+        dt = stage2_dt<CG>(a, threadIdx.x == 0 && bx == 0 && by == 0 && b == 0);
         hdt = 0.5f * dt;
-        if (threadIdx.x == 0 && bx == 0 && by == 0 && b == 0) {
-            uint32_t st_bits = 0;
-            if (!isfinite(dt)) st_bits |= SWE_S_NONFINITE_DT;
-            else if (!(dt > 0.0f)) st_bits |= SWE_S_NONPOSITIVE_DT;
-            if (st_bits) atomicOr(&a.red[2], st_bits);
-            a.red[3] = f2u(dt);
-        }
     }
 
     const bool wsr = a.wsr != 0;
@@ -469,7 +339,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs& a, int bx, int by, in
     for (int k = j0 - 2, it = 0; k < jend + 2; ++k, ++it) {
         State s, ur;
         float z;
-        sweep_cell<STAGE, CG>(a, b, k, c, hdt, s, z, ur);
+        sweep_cell<STAGE, CG, ExactPredict>(a, b, k, c, hdt, s, z, ur);
         if (STAGE == 1 && (unsigned)k < (unsigned)a.ny && (unsigned)c < (unsigned)a.nx)
             bad |= !(isfinite(s.h) && isfinite(s.hu) && isfinite(s.hv));
         pm2 = pm1;
@@ -558,238 +428,20 @@ __global__ void __launch_bounds__(SW_WARPS * 32, 8) sweep_kernel(const StepArgs 
 }
 
 
-// ---------------------------------------------------------------------------
-// Persistent ensemble kernel: many independent scenarios of different grid
-// sizes, each with its own time step, boundary series and step count, in
-// one launch.
-//
-// Work item = (scenario, phase, tile); phase 2n is stage 1 of step n, phase
-// 2n+1 its stage 2.  Each scenario keeps a 64-bit claim word (phase << 32 |
-// tiles claimed) and a done counter.  A block claims a tile with one
-// atomicAdd on the claim word; when the phase is fully claimed it tries the
-// next scenario.  The block that completes a phase's last tile advances the
-// scenario (time, step count, next boundary level, cleared reductions) and
-// publishes the next phase with atomicExch.  No block ever waits for a
-// particular item, so the kernel cannot deadlock; idle polling is bounded
-// (EnsIdleLimit polls with __nanosleep back-off) after which the kernel sets
-// an error bit and returns.  State written by other blocks is read through
-// L2 (ld.global.cg); writes are fenced before a phase is published.
-struct EnsCtl {
-    unsigned long long claim;  // phase << 32 | tiles claimed
-    unsigned int done;         // tiles finished in the current phase
-    unsigned int red[SWE_RED_WORDS];
-    float level;               // boundary level of the current step
-    int step;                  // steps completed
-    int finished;              // 0 running, 1 done, 2 failed
-    int tiles, nbx, rows, steps;
-    int nseries;
-    float dt_last;
-    unsigned int status;
-    double time;               // simulated time since the start
-    double start;
-    const float* series_t;
-    const float* series_w;
-    float* Ua;                 // state buffers: step n reads U[n & 1]
-    float* Ub;
-    // interval mode (n_out > 0)
-    double out_dt, elapsed, tol, cap;
-    int n_out, chunk, ngauge, nx;
-    float max_dt_cur;          // max_dt of the current step (both modes)
-    const float* out_levels;
-    const int32_t* gauge_cells;
-    float* gauge_out;
-    const float* bed;
-};
-
-struct EnsGlobal {
-    unsigned int finished;  // scenarios done or failed
-    unsigned int error;     // bit 1: no progress within EnsStallNs
-    unsigned int progress;  // phases completed, all scenarios
-    unsigned int pad[13];
-};
-
-// An idle block gives up (error bit 1) only when no scenario has completed
-// a phase for this long; phases complete in microseconds to milliseconds.
-constexpr unsigned long long EnsStallNs = 2000000000ull;
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ float ens_level(const EnsCtl& c) {
-    if (c.nseries <= 0) return c.level;
-    const float t = (float)(c.start + c.time);
-    const float* times = c.series_t;
-    const float* levels = c.series_w;
-    const int n = c.nseries;
-    if (n == 1) return levels[0];
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (times[mid] < t) lo = mid + 1;
-        else hi = mid;
+// Persistent ensemble kernel (scheduler in swe_ensemble.cuh) over the IEEE
+// sweep tiles.
+struct ExactTile {
+    template <int STAGE, int FRIC>
+    static __device__ __forceinline__ void run(const StepArgs& a, int bx, int by, int rows) {
+        sweep_tile<STAGE, FRIC, true>(a, bx, by, 0, rows);
     }
-    const int idx = min(max(lo, 1), n - 1);
-    const float t0 = times[idx - 1], t1 = times[idx];
-    const float weight = __fdiv_rn(t - t0, fmaxf(t1 - t0, 1.1920929e-07f));
-    return levels[idx - 1] + weight * (levels[idx] - levels[idx - 1]);
-}
-
-// Thread 0 of the block that finished the last tile of `phase`.
-__device__ void ens_advance(EnsCtl* c, EnsGlobal* g, unsigned int phase) {
-    __threadfence();
-    c->done = 0u;
-    const unsigned int st = __ldcg(&c->red[2]);
-    if ((phase & 1u) == 0u) {  // stage 1 done: stage 2 derives dt from red
-        if (st & SWE_S_NONFINITE_STATE) {
-            c->status = st;
-            c->finished = 2;
-            __threadfence();
-            atomicAdd(&g->finished, 1u);
-            atomicAdd(&g->progress, 1u);
-            return;
-        }
-    } else {  // stage 2 done: the step is complete
-        const float dt = __uint_as_float(__ldcg(&c->red[3]));
-        if (st & (SWE_S_NONFINITE_DT | SWE_S_NONPOSITIVE_DT)) {
-            c->status = st;
-            c->finished = 2;
-            __threadfence();
-            atomicAdd(&g->finished, 1u);
-            atomicAdd(&g->progress, 1u);
-            return;
-        }
-        c->time += (double)dt;
-        c->dt_last = dt;
-        const int done_step = c->step;
-        c->step = done_step + 1;
-        int fin = 0;
-        if (c->n_out > 0) {
-            // the interval bookkeeping of swe_run_clock_f32 (solver.py:741-768)
-            double el = c->elapsed + (double)dt;
-            if (el > c->out_dt && el - c->out_dt <= c->tol) el = c->out_dt;
-            if (c->out_dt - el <= c->tol) {
-                const float* Unew = (done_step & 1) ? c->Ua : c->Ub;  // this step's output
-                for (int q = 0; q < c->ngauge; ++q) {
-                    const size_t cell = (size_t)c->gauge_cells[2 * q] * c->nx + c->gauge_cells[2 * q + 1];
-                    c->gauge_out[(size_t)c->chunk * c->ngauge + q] = __ldcg(Unew + cell) + c->bed[cell];
-                }
-                c->chunk += 1;
-                el = 0.0;
-                if (c->chunk >= c->n_out) fin = 1;
-            }
-            c->elapsed = el;
-            if (!fin && c->step >= c->steps) {
-                c->status = SWE_S_STEP_LIMIT;
-                fin = 2;
-            }
-            if (!fin) {
-                const double rem = c->out_dt - el;
-                c->max_dt_cur = (float)((c->cap > 0.0 && c->cap < rem) ? c->cap : rem);
-                c->level = c->out_levels[c->chunk];
-            }
-        } else {
-            if (c->step >= c->steps) fin = 1;
-            else c->level = ens_level(*c);
-        }
-        if (fin) {
-            c->finished = fin;
-            __threadfence();
-            atomicAdd(&g->finished, 1u);
-            atomicAdd(&g->progress, 1u);
-            return;
-        }
-        for (int w = 0; w < SWE_RED_WORDS; ++w) c->red[w] = 0u;
-    }
-    __threadfence();
-    atomicExch(&c->claim, (unsigned long long)(phase + 1u) << 32);
-    atomicAdd(&g->progress, 1u);
-}
+};
 
 template <int FRIC>
 __global__ void __launch_bounds__(SW_WARPS * 32, 6)
-ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGlobal* g) {
-    __shared__ StepArgs sa;
-    __shared__ int s_item[3];
-    int rr = (int)(blockIdx.x % (unsigned)count);
-    unsigned int seen_progress = 0xffffffffu, backoff = 64;
-    unsigned long long seen_at = 0;
-    while (true) {
-        __syncthreads();  // everyone is done with the previous item's shared data
-        if (threadIdx.x == 0) {
-            int item = -2, phase = 0, tile = 0;
-            for (int k = 0; k < count && item == -2; ++k) {
-                const int sidx = (rr + k) % count;
-                EnsCtl* c = ctl + sidx;
-                if (*(volatile int*)&c->finished) continue;
-                const unsigned long long old = atomicAdd(&c->claim, 1ull);
-                const unsigned int ph = (unsigned int)(old >> 32), cl = (unsigned int)old;
-                if (cl < (unsigned int)c->tiles) {
-                    item = sidx;
-                    phase = (int)ph;
-                    tile = (int)cl;
-                    rr = sidx;
-                }
-            }
-            if (item == -2) {
-                const unsigned int prog = *(volatile unsigned int*)&g->progress;
-                const unsigned long long now = global_ns();
-                if (*(volatile unsigned int*)&g->finished >= (unsigned int)count ||
-                    *(volatile unsigned int*)&g->error) {
-                    item = -1;
-                } else if (prog != seen_progress) {
-                    seen_progress = prog;
-                    seen_at = now;
-                    __nanosleep(backoff);
-                } else if (now - seen_at > EnsStallNs) {
-                    atomicOr(&g->error, 1u);
-                    item = -1;
-                } else {
-                    __nanosleep(backoff);
-                    backoff = min(backoff * 2u, 4096u);
-                }
-            } else {
-                backoff = 64;
-                __threadfence();
-            }
-            s_item[0] = item;
-            s_item[1] = phase;
-            s_item[2] = tile;
-        }
-        __syncthreads();
-        const int sidx = s_item[0];
-        if (sidx == -1) return;
-        if (sidx == -2) continue;
-        const int phase = s_item[1], tile = s_item[2];
-        // this scenario's arguments, with the state buffers of this step
-        {
-            const int* src = reinterpret_cast<const int*>(args + sidx);
-            int* dst = reinterpret_cast<int*>(&sa);
-            for (int w = threadIdx.x; w < (int)(sizeof(StepArgs) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
-        }
-        __syncthreads();
-        const EnsCtl* c = ctl + sidx;
-        const int step = phase >> 1;
-        if (threadIdx.x == 0) {
-            sa.U = (step & 1) ? c->Ub : c->Ua;
-            sa.U_out = (step & 1) ? c->Ua : c->Ub;
-            sa.max_dt = __ldcg(&c->max_dt_cur);
-        }
-        __syncthreads();
-        const int nbx = c->nbx, rows = c->rows;
-        const int bx = tile % nbx, by = tile / nbx;
-        if ((phase & 1) == 0) sweep_tile<1, 0, true>(sa, bx, by, 0, rows);
-        else sweep_tile<2, FRIC, true>(sa, bx, by, 0, rows);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            EnsCtl* cw = ctl + sidx;
-            const unsigned int d = atomicAdd(&cw->done, 1u);
-            if (d + 1u == (unsigned int)cw->tiles) ens_advance(cw, g, (unsigned int)phase);
-        }
-    }
+ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGlobal* g,
+                unsigned long long stall_ns) {
+    ensemble_body<FRIC, ExactTile>(args, ctl, count, g, stall_ns);
 }
 
 // One block of >= count threads (count <= 1024).
@@ -908,6 +560,7 @@ extern "C" int swe_spatial_operator_f32(const float* U, const float* bed, int B,
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess) return SWE_ECUDA;
     // the stage-1 kernel of the step computes exactly this (tendency + maxima)
+    if (p->arithmetic == SWE_ARITH_FAST) return fast_launch_stages(1, a, sweep_grid_of(a), s);
     if (use_tiled_kernels()) stage_kernel<1><<<grid_of(a), NT, 0, s>>>(a);
     else sweep_kernel<1, 0><<<sweep_grid_of(a), SW_WARPS * 32, 0, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
@@ -918,20 +571,24 @@ namespace {
 
 int launch_step(int stage, const float* U, const float* bed, int bedB, const float* n, int nB, int B,
                 int ny, int nx, const swe_params* p, const float* level, int levelB, float max_dt,
-                const swe_clock* clk, const float* infil, int infil_mode, int infil_batch,
-                float* scratch_k, uint32_t* red, float* U_out, float* hmax, void* stream) {
+                const swe_clock* clk, const float* rain, int rain_mode, int rain_batch,
+                const float* infil, int infil_mode, int infil_batch, float* scratch_k, uint32_t* red,
+                float* U_out, float* hmax, void* stream) {
     StepArgs a{};
     if (stage != 1 && stage != 2 && stage != 3) return SWE_EARG;
     if (!fill_common(a, U, bed, B, bedB, ny, nx, p, level, levelB)) return SWE_EARG;
     if (!scratch_k || !red || !U_out || (p->apply_friction && !n)) return SWE_EARG;
     if (p->apply_friction && nB != 1 && nB != B) return SWE_EARG;
     if (!valid_forcing(infil, infil_mode, infil_batch, B)) return SWE_EARG;
+    if (!valid_forcing(rain, rain_mode, rain_batch, B)) return SWE_EARG;
     a.n = n;
     a.nB = nB;
     a.infil = infil;
     a.infil_mode = infil_mode;
     a.infil_batch = infil_batch;
-    a.rain_mode = SWE_FORCING_NONE;
+    a.rain = rain;
+    a.rain_mode = rain_mode;
+    a.rain_batch = rain_batch;
     a.tend = scratch_k;
     a.U_out = U_out;
     a.red = red;
@@ -939,12 +596,14 @@ int launch_step(int stage, const float* U, const float* bed, int bedB, const flo
     a.clk = clk;
     a.hmax = hmax;
     cudaStream_t s = (cudaStream_t)stream;
-    const bool tiled = use_tiled_kernels();
+    const bool fast = p->arithmetic == SWE_ARITH_FAST;
+    const bool tiled = !fast && use_tiled_kernels();
     const dim3 g = tiled ? grid_of(a) : sweep_grid_of(a);
+    // A clocked step's reduction words are cleared by swe_clock_f32.
+    if ((stage & 1) && !clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
+        return SWE_ECUDA;
+    if (fast) return fast_launch_stages(stage, a, g, s);
     if (stage & 1) {
-        // A clocked step's reduction words are cleared by swe_clock_f32.
-        if (!clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
-            return SWE_ECUDA;
         if (tiled) stage_kernel<1><<<g, NT, 0, s>>>(a);
         else sweep_kernel<1, 0><<<g, SW_WARPS * 32, 0, s>>>(a);
     }
@@ -972,7 +631,20 @@ extern "C" int swe_step_stage_f32(int stage, const float* U, const float* bed, i
                                   int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                                   void* stream) {
     return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt, nullptr,
-                       infil, infil_mode, infil_batch, scratch_k, red, U_out, nullptr, stream);
+                       nullptr, SWE_FORCING_NONE, 1, infil, infil_mode, infil_batch, scratch_k, red,
+                       U_out, nullptr, stream);
+}
+
+extern "C" int swe_step_stage_forced_f32(int stage, const float* U, const float* bed, int bedB,
+                                         const float* n, int nB, int B, int ny, int nx,
+                                         const swe_params* p, const float* level, int levelB,
+                                         float max_dt, const float* rain, int rain_mode,
+                                         int rain_batch, const float* infil, int infil_mode,
+                                         int infil_batch, float* scratch_k, uint32_t* red,
+                                         float* U_out, void* stream) {
+    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, max_dt, nullptr,
+                       rain, rain_mode, rain_batch, infil, infil_mode, infil_batch, scratch_k, red,
+                       U_out, nullptr, stream);
 }
 
 extern "C" int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB,
@@ -982,8 +654,9 @@ extern "C" int swe_step_clocked_f32(int stage, const float* U, const float* bed,
                                     int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                                     float* hmax, void* stream) {
     if (!clock) return SWE_EARG;
-    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, 0.0f, clock, infil,
-                       infil_mode, infil_batch, scratch_k, red, U_out, hmax, stream);
+    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, 0.0f, clock, nullptr,
+                       SWE_FORCING_NONE, 1, infil, infil_mode, infil_batch, scratch_k, red, U_out, hmax,
+                       stream);
 }
 
 extern "C" int swe_step_f32(const float* U, const float* bed, int bedB, const float* n, int nB,
@@ -1087,12 +760,13 @@ extern "C" int swe_ensemble_prepare_f32(const swe_ensemble_member* members, int 
     EnsCtl* ctl_dev = (EnsCtl*)(ws + ens_offset_ctl(count));
     int rc = SWE_OK;
     const int fric0 = members[0].params.apply_friction ? 1 + members[0].params.friction_model : 0;
+    const int arith0 = members[0].params.arithmetic;
     for (int m = 0; m < count && rc == SWE_OK; ++m) {
         const swe_ensemble_member& e = members[m];
         StepArgs a{};
         const int fric = e.params.apply_friction ? 1 + e.params.friction_model : 0;
         const bool interval = e.n_out > 0;
-        if (fric != fric0 || !e.U_a || !e.U_b || !e.k1 || e.steps < 0 || e.rows < 1 ||
+        if (fric != fric0 || e.params.arithmetic != arith0 || !e.U_a || !e.U_b || !e.k1 || e.steps < 0 || e.rows < 1 ||
             (!interval && e.nseries > 0 && (!e.series_t || !e.series_w)) || e.n_out < 0 ||
             (interval && (!(e.out_dt > 0.0) || !e.out_levels || e.ngauge < 0 ||
                           (e.ngauge > 0 && (!e.gauge_cells || !e.gauge_out)))) ||
@@ -1173,18 +847,22 @@ extern "C" int swe_ensemble_reset_f32(void* workspace, int count, void* stream) 
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
-extern "C" int swe_ensemble_run_f32(void* workspace, int count, int friction, int blocks,
-                                    void* stream) {
-    if (!workspace || count < 1 || count > 1024 || blocks < 1 || friction < 0 || friction > 2)
+extern "C" int swe_ensemble_run_f32(void* workspace, int count, int friction, int arithmetic,
+                                    int blocks, long long stall_ns, void* stream) {
+    if (!workspace || count < 1 || count > 1024 || blocks < 1 || friction < 0 || friction > 2 ||
+        (arithmetic != SWE_ARITH_EXACT && arithmetic != SWE_ARITH_FAST) || stall_ns < 0)
         return SWE_EARG;
     char* ws = (char*)workspace;
     const StepArgs* args = (const StepArgs*)ws;
     EnsCtl* ctl = (EnsCtl*)(ws + ens_offset_ctl(count));
     EnsGlobal* g = (EnsGlobal*)(ws + ens_offset_global(count));
     cudaStream_t s = (cudaStream_t)stream;
-    if (friction == 0) ensemble_kernel<0><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
-    else if (friction == 1) ensemble_kernel<1><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
-    else ensemble_kernel<2><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g);
+    const unsigned long long limit = stall_ns > 0 ? (unsigned long long)stall_ns : EnsStallNsDefault;
+    if (arithmetic == SWE_ARITH_FAST)
+        return fast_launch_ensemble(friction, blocks, args, ctl, count, g, limit, s);
+    if (friction == 0) ensemble_kernel<0><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g, limit);
+    else if (friction == 1) ensemble_kernel<1><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g, limit);
+    else ensemble_kernel<2><<<blocks, SW_WARPS * 32, 0, s>>>(args, ctl, count, g, limit);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
@@ -1237,5 +915,5 @@ extern "C" int swe_load_kernels(void) {
     };
     for (const void* f : fns)
         if (cudaFuncGetAttributes(&at, f) != cudaSuccess) return SWE_ECUDA;
-    return SWE_OK;
+    return fast_load_kernels();
 }

@@ -29,6 +29,8 @@ class EnsembleResult:
     hmax: Optional[List[torch.Tensor]]
     elapsed_ms: float            # device time of the persistent launch
     cell_updates: int
+    failed: List[int]            # scenarios whose time step failed (run(strict=False))
+    status: List[int]            # SWE_S_* bits of each scenario (0: no failure)
 
     @property
     def mcells_per_s(self) -> float:
@@ -40,11 +42,20 @@ class Ensemble:
 
     ``rows`` fixes the sweep tile height of every scenario; by default it is
     the autotuner's ensemble value (``autotune.tuned_ensemble_rows``).
+    ``arithmetic`` selects the step kernels ("exact": IEEE operation for
+    operation as the reference; "fast": the tolerance mode).  ``stall_ns``
+    is the persistent kernel's idle limit (None: the library's 2 s): a launch
+    in which no scenario completes a phase for that long stops with an error.
     """
 
     def __init__(self, scenarios: Sequence, device="cuda", steps: Optional[int] = None,
-                 rows: Optional[int] = None, track_hmax: bool = False, max_dt: float = 1.0e9):
+                 rows: Optional[int] = None, track_hmax: bool = False, max_dt: float = 1.0e9,
+                 arithmetic: str = "exact", stall_ns: Optional[int] = None):
         from .autotune import tuned_ensemble_rows
+        self.arith = nat.arithmetic_code(arithmetic)
+        self.stall_ns = 0 if stall_ns is None else int(stall_ns)
+        if self.stall_ns < 0:
+            raise ValueError("stall_ns must be positive")
         self.device = torch.device(device)
         self.count = len(scenarios)
         if not 1 <= self.count <= 1024:
@@ -77,7 +88,7 @@ class Ensemble:
                 sw = torch.as_tensor(sc.bc_levels, dtype=torch.float32, device=dev).contiguous()
                 nser = st.numel()
             steps_m = int(sc.steps if steps is None else steps)
-            r = int(rows) if rows is not None else tuned_ensemble_rows(dev)
+            r = int(rows) if rows is not None else tuned_ensemble_rows(dev, arithmetic)
             mem = members[m]
             mem.bed, mem.n = bed.data_ptr(), n.data_ptr()
             mem.U_a, mem.U_b, mem.k1 = Ua.data_ptr(), Ub.data_ptr(), k1.data_ptr()
@@ -88,7 +99,7 @@ class Ensemble:
             mem.level = float(cfg.constant_level)
             mem.start_time = 0.0
             mem.max_dt = float(max_dt)
-            mem.params = nat.params(cfg, sc.dx, sc.dy)
+            mem.params = nat.params(cfg, sc.dx, sc.dy, arithmetic)
             self._keep += [bed, n, Ua, Ub, k1, hm, st, sw]
             self.U_a.append(Ua)
             self.U_b.append(Ub)
@@ -116,10 +127,14 @@ class Ensemble:
         lib, st = nat.lib(), nat.stream_handle(self.device)
         nat.check(lib.swe_ensemble_reset_f32(nat.ptr(self.workspace), self.count, st), "ensemble reset")
         nat.check(lib.swe_ensemble_run_f32(nat.ptr(self.workspace), self.count, self.friction,
-                                           self.blocks, st), "ensemble run")
+                                           self.arith, self.blocks, self.stall_ns, st), "ensemble run")
 
-    def run(self) -> EnsembleResult:
-        """Run every scenario from its initial state; returns final states."""
+    def run(self, strict: bool = True) -> EnsembleResult:
+        """Run every scenario from its initial state; returns final states.
+
+        A scenario whose time step fails (non-finite state or dt) stops on
+        its own; the others run to the end.  With ``strict`` the failure
+        raises FloatingPointError, otherwise it is listed in ``failed``."""
         for Ua, U0 in zip(self.U_a, self.initial):
             Ua.copy_(U0)
         for hm, U0 in zip(self.hmax, self.initial):
@@ -145,11 +160,14 @@ class Ensemble:
         res = (nat.SweEnsembleResult * self.count).from_buffer_copy(raw)
         if int(self.error_dev.item()) != 0:
             raise RuntimeError("ensemble kernel stopped: idle limit reached")
-        states, steps, times = [], [], []
+        states, steps, times, failed, status = [], [], [], [], []
         for m in range(self.count):
             r = res[m]
             if r.finished == 2:
-                raise FloatingPointError(f"scenario {m}: time step failed (status {r.status})")
+                if strict:
+                    raise FloatingPointError(f"scenario {m}: time step failed (status {r.status})")
+                failed.append(m)
+            status.append(int(r.status))
             buf = self.U_a[m] if r.steps % 2 == 0 else self.U_b[m]
             states.append(buf.clone().unsqueeze(0))
             steps.append(int(r.steps))
@@ -157,7 +175,7 @@ class Ensemble:
         hmax = [h.clone() if h is not None else None for h in self.hmax] if any(
             h is not None for h in self.hmax) else None
         total = sum(c * s for c, s in zip(self.cells, steps))
-        return EnsembleResult(states, steps, times, hmax, e0.elapsed_time(e1), total)
+        return EnsembleResult(states, steps, times, hmax, e0.elapsed_time(e1), total, failed, status)
 
 
 @dataclass
@@ -189,8 +207,10 @@ class GaugeEnsemble:
 
     def __init__(self, bed: torch.Tensor, n: torch.Tensor, U0: torch.Tensor, out_levels: torch.Tensor,
                  out_dt: float, gauges: Sequence, config: SWEConfig, dx: float, dy: Optional[float] = None,
-                 rows: Optional[int] = None, max_steps: int = 1 << 30, max_dt_cap: float = 0.0):
+                 rows: Optional[int] = None, max_steps: int = 1 << 30, max_dt_cap: float = 0.0,
+                 arithmetic: str = "exact"):
         from .autotune import tuned_ensemble_rows
+        self.arith = nat.arithmetic_code(arithmetic)
         M, ny, nx = bed.shape
         if not 1 <= M <= 1024:
             raise ValueError("a gauge ensemble holds 1 to 1024 members")
@@ -221,8 +241,8 @@ class GaugeEnsemble:
                                   device=dev)
         self.gauge_out = torch.zeros((M, self.n_out, max(self.ngauge, 1)), device=dev)
         self.friction = (1 + (0 if config.frictionmodel == "manning" else 1)) if config.apply_friction else 0
-        r = int(rows) if rows is not None else tuned_ensemble_rows(dev)
-        p = nat.params(config, dx, dx if dy is None else dy)
+        r = int(rows) if rows is not None else tuned_ensemble_rows(dev, arithmetic)
+        p = nat.params(config, dx, dx if dy is None else dy, arithmetic)
         members = (nat.SweEnsembleMember * M)()
         for m in range(M):
             mem = members[m]
@@ -258,8 +278,8 @@ class GaugeEnsemble:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         nat.check(lib.swe_ensemble_reset_f32(nat.ptr(self.workspace), self.M, st), "ensemble reset")
         e0.record()
-        nat.check(lib.swe_ensemble_run_f32(nat.ptr(self.workspace), self.M, self.friction, self.blocks,
-                                           st), "ensemble run")
+        nat.check(lib.swe_ensemble_run_f32(nat.ptr(self.workspace), self.M, self.friction, self.arith,
+                                           self.blocks, 0, st), "ensemble run")
         e1.record()
         nat.check(lib.swe_ensemble_results_f32(nat.ptr(self.workspace), self.M,
                                                nat.ptr(self.results_dev), nat.ptr(self.error_dev), st),

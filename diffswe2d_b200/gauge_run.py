@@ -94,7 +94,7 @@ class GaugeRunWorkspace:
         self.store, self.store_k1 = [], []
         self.stored = False
         from .autotune import tuned_rows_for_shape
-        self.rows = tuned_rows_for_shape(B, ny, nx, dev)
+        self.rows = tuned_rows_for_shape(B, ny, nx, dev, arithmetic=model.arithmetic)
 
     # ------------------------------------------------------------ launches
     def _tick(self, state):

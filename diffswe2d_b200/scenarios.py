@@ -159,3 +159,42 @@ def ensemble_member(ny: int, nx: int, seed: int) -> Scenario:
     return Scenario(f"ensemble_{ny}x{nx}_{seed}", z.astype(np.float32),
                     np.full_like(z, manning, np.float32), U0.astype(np.float32), dx, dx, cfg,
                     times, levels, steps=2000, meta=dict(seed=seed, hump=bool(hump)))
+
+
+def spun_up(base: Scenario, seconds: float, device="cuda", arithmetic: str = "exact") -> Scenario:
+    """The scenario advanced ``seconds`` of simulated time by ``SWE2D.forward``
+    on the GPU (its boundary series included), as a new scenario whose
+    initial state is that state and whose ``meta["start_time"]`` is
+    ``seconds``: a state with waves and moving wet/dry fronts instead of
+    water at rest, e.g. to tile into the 4096x4096 throughput workload."""
+    import torch
+
+    from .config import SWEConfig
+    from .solver import SWE2D
+    dev = torch.device(device)
+    model = SWE2D(torch.from_numpy(base.bed).to(dev), torch.from_numpy(base.roughness).to(dev),
+                  base.dx, base.dy, config=SWEConfig(**base.config), train_dem=False,
+                  arithmetic=arithmetic)
+    if base.bc_times is not None:
+        model.set_dynamic_boundary(torch.from_numpy(base.bc_times).to(dev),
+                                   torch.from_numpy(base.bc_levels).to(dev))
+    with torch.no_grad():
+        U, _ = model(torch.from_numpy(base.U0).to(dev), t_end=float(seconds), start_time=0.0)
+    U0 = U.cpu().numpy().astype(np.float32)
+    return Scenario(f"{base.name}_at_{seconds:g}s", base.bed, base.roughness, U0, base.dx, base.dy,
+                    dict(base.config), base.bc_times, base.bc_levels, base.steps,
+                    dict(base.meta, start_time=float(seconds), spun_up_from=base.name))
+
+
+#: simulated seconds of the runup scenario before it is tiled into the
+#: throughput workload: the N-wave's trough has run down the beach and its
+#: crest is arriving (waves and wet/dry fronts across the domain)
+WORKLOAD_SPIN_UP_S = 8.0
+
+
+def throughput_workload(ny: int = 4096, nx: int = 4096, device="cuda") -> Scenario:
+    """The 4096x4096 throughput workload: the 244x393 runup scenario (seed 0)
+    spun up for WORKLOAD_SPIN_UP_S seconds with the IEEE kernels, then tiled
+    (bed, roughness and state) to ny x nx."""
+    base = spun_up(runup(seed=0), WORKLOAD_SPIN_UP_S, device)
+    return tiled(base, ny, nx)

@@ -12,6 +12,7 @@ from __future__ import annotations
 from numbers import Integral, Real
 from typing import Optional, Union
 
+import numpy as np
 import torch
 import torch.nn as nn
 
@@ -26,11 +27,23 @@ class SWE2D(nn.Module):
 
     ``forward(..., t_end=...)`` interprets ``t_end`` as the duration of that
     call, as the reference does (``src/solver.py:40-47``).
+
+    ``arithmetic`` (not in the reference) selects the step kernels: "exact"
+    evaluates every float32 operation of the reference's step in its order
+    with IEEE rounding; "fast" is the tolerance mode (fused multiply-adds,
+    hardware approximations, about three times the throughput), within FP32
+    rounding of the reference.  ``rainfall`` is an object with
+    ``at(time) -> rate`` (``RainfallForcing``); as in the reference, stage 1
+    of a step uses the rate at the step's start and stage 2 the rate half a
+    step later, so a step with rainfall reads dt between its two kernels.
     """
 
     def __init__(self, bed_reference, roughness_length, dx, dy, config=None, train_dem=True,
-                 maximum_dem_correction=None, valid_mask=None, x=None, y=None, rainfall=None):
+                 maximum_dem_correction=None, valid_mask=None, x=None, y=None, rainfall=None,
+                 arithmetic="exact"):
         super().__init__()
+        nat.arithmetic_code(arithmetic)
+        self.arithmetic = arithmetic
         self.cfg = config or SWEConfig()
         self.dx, self.dy = float(dx), float(dy)
         if self.dx <= 0.0 or self.dy <= 0.0:
@@ -167,7 +180,7 @@ class SWE2D(nn.Module):
 
     # ------------------------------------------------------ argument packing
     def _params(self):
-        return nat.params(self.cfg, self.dx, self.dy)
+        return nat.params(self.cfg, self.dx, self.dy, self.arithmetic)
 
     @staticmethod
     def _level_arg(level: torch.Tensor, batch: int):
@@ -275,6 +288,9 @@ class SWE2D(nn.Module):
         """
         self._check_state(U)
         if self._needs_adjoint(U, boundary_level):
+            if self.rainfall is not None:
+                raise NotImplementedError("the step adjoint has no rainfall source; differentiate "
+                                          "a model without rainfall")
             from .adjoint import step_with_adjoint
             return step_with_adjoint(self, U, model_time, max_dt, infiltration, boundary_level)
         U = nat.require_cuda_f32("U", U)
@@ -283,7 +299,12 @@ class SWE2D(nn.Module):
                           else torch.tensor(float(max_dt), dtype=torch.float32)).item())
         level = self._prepare_boundary_level(
             self.cfg.constant_level if boundary_level is None else boundary_level, U)
-        U_new, status, dt = self._launch_step(U, level, max_dt_f, infiltration)
+        if self.rainfall is not None:
+            # model_time is taken in U's dtype first (src/solver.py:593-597, :608)
+            time_float = float(np.float32(self._scalar_float(model_time, "model_time")))
+            U_new, status, dt = self._launch_step_rain(U, level, max_dt_f, infiltration, time_float)
+        else:
+            U_new, status, dt = self._launch_step(U, level, max_dt_f, infiltration)
         self._raise_on_status(status, dt)
         return U_new, dt
 
@@ -316,6 +337,54 @@ class SWE2D(nn.Module):
         status = int(host[0].item()) & 0xFFFFFFFF
         dt = float(host[1:2].view(torch.float32).item())
         return U_out, status, dt
+
+    def _host_dt(self, red_host: torch.Tensor, max_dt_f: float) -> float:
+        """The step's dt from the stage-1 maxima, in float32 as the kernels and
+        the reference compute it (src/solver.py:620-626)."""
+        ax, ay = (float(v) for v in red_host[0:2].view(torch.float32))
+        f = np.float32
+        den = max(f(f(ax) / f(self.dx)) + f(f(ay) / f(self.dy)), f(self.cfg.epsilon))
+        stable = f(f(1.0) / f(den)) * f(self.cfg.cfl)
+        return float(stable if np.isnan(stable) else min(stable, f(max_dt_f)))
+
+    def _launch_step_rain(self, U, level, max_dt_f, infiltration, time_float):
+        """One step with the rainfall source: stage 1 with the rate at the
+        step's start, dt read on the host, stage 2 with the rate at t + dt/2
+        (src/solver.py:609-643)."""
+        B, _, ny, nx = U.shape
+        bed, n = self._fields(U)
+        lv, levelB = self._level_arg(level, B)
+        h = U[:, 0:1]
+        infil, imode, iB = self._forcing_arg(infiltration, h)
+        U_out = torch.empty_like(U)
+        scratch = torch.empty_like(U)
+        red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=U.device)
+        p = self._params()
+        st = nat.stream_handle(U.device)
+        lib = nat.lib()
+
+        def stage(k, rate):
+            rain, rmode, rB = self._forcing_arg(rate, h)
+            rc = lib.swe_step_stage_forced_f32(
+                k, nat.ptr(U), nat.ptr(bed), bed.shape[0], nat.ptr(n), n.shape[0], B, ny, nx, p,
+                nat.ptr(lv), levelB, max_dt_f, nat.ptr(rain), rmode, rB, nat.ptr(infil), imode, iB,
+                nat.ptr(scratch), nat.ptr(red), nat.ptr(U_out), st)
+            nat.check(rc, "step")
+            return rain  # kept alive until the kernel has read it
+
+        keep = stage(1, self.rainfall.at(time_float))
+        host = red.cpu()
+        status = int(host[2].item()) & 0xFFFFFFFF
+        if status & nat.S_NONFINITE_STATE:
+            return U_out, status, float("nan")
+        dt = self._host_dt(host, max_dt_f)
+        if not np.isfinite(dt) or not dt > 0.0:
+            return U_out, nat.S_NONFINITE_DT if not np.isfinite(dt) else nat.S_NONPOSITIVE_DT, dt
+        keep = stage(2, self.rainfall.at(time_float + 0.5 * dt))
+        host = red[2:4].cpu()
+        del keep
+        status = int(host[0].item()) & 0xFFFFFFFF
+        return U_out, status, float(host[1:2].view(torch.float32).item())
 
     @staticmethod
     def _raise_on_status(status: int, dt: float) -> None:
@@ -388,6 +457,8 @@ class SWE2D(nn.Module):
         """The device loop serves forward() calls that need no host work per
         step: no callback, no autograd, and a positive max_dt cap if any."""
         if callback is not None or not U0.is_cuda or U0.dtype != torch.float32:
+            return False
+        if self.rainfall is not None:  # rates are evaluated on the host per stage
             return False
         if self._needs_adjoint(U0, boundary_level) or (
                 torch.is_grad_enabled() and boundary_level is None and self.use_dynamic_bc
@@ -510,6 +581,7 @@ class _DeviceLoop:
         self.clock = torch.zeros(72, dtype=torch.uint8, device=dev)
         self.clock_host = torch.zeros(72, dtype=torch.uint8).pin_memory()
         self.params = params
+        self.arithmetic = model.arithmetic
         self.B, self.ny, self.nx, self.levelB, self.dev = B, ny, nx, levelB, dev
         self.graph = None
 
@@ -549,7 +621,8 @@ class _DeviceLoop:
         if self.graph is None:
             from .autotune import sweep_rows, tuned_rows_for_shape
             nat.load_kernels()
-            rows = tuned_rows_for_shape(self.B, self.ny, self.nx, self.dev)
+            rows = tuned_rows_for_shape(self.B, self.ny, self.nx, self.dev,
+                                        arithmetic=self.arithmetic)
             graph = torch.cuda.CUDAGraph()
             with sweep_rows(rows), torch.cuda.graph(graph):
                 for s in range(self.chunk):

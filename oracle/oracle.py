@@ -231,18 +231,26 @@ class Oracle:
                                        ctypes.c_double(dry_depth), ctypes.c_double(epsilon), _ptr(out))
         return out
 
-    # src/solver.py:572 (array part): returns (U_new, dt in working precision)
-    def step(self, U, bed, n, cfg, dx, dy, level, max_dt, infil=None):
+    # src/solver.py:572 (array part): returns (U_new, dt in working precision).
+    # rain0 / rain1: rainfall rates of stage 1 / stage 2 (broadcast to [B,1,ny,nx]).
+    def step(self, U, bed, n, cfg, dx, dy, level, max_dt, infil=None, rain0=None, rain1=None):
         U, bed, n = _arr(U, self.dtype), _arr(bed, self.dtype), _arr(n, self.dtype)
         B, _, ny, nx = U.shape
         out = np.empty_like(U)
         dt = self._scalar(0)
         p = make_params(cfg, dx, dy)
         lv = _batch_values(level, B, self.dtype)
-        inf = None if infil is None else _arr(np.broadcast_to(infil, (B, 1, ny, nx)), self.dtype)
-        rc = self._fn("step")(_ptr(U), _ptr(bed), bed.shape[0], _ptr(n), n.shape[0], B, ny, nx,
-                              ctypes.byref(p), _ptr(lv), self._scalar(_f(self.dtype, max_dt)),
-                              None if inf is None else _ptr(inf), _ptr(out), ctypes.byref(dt))
+
+        def field(a):
+            return None if a is None else _arr(np.broadcast_to(a, (B, 1, ny, nx)), self.dtype)
+
+        inf, r0, r1 = field(infil), field(rain0), field(rain1)
+        rc = self._fn("step_forced")(_ptr(U), _ptr(bed), bed.shape[0], _ptr(n), n.shape[0], B, ny,
+                                     nx, ctypes.byref(p), _ptr(lv),
+                                     self._scalar(_f(self.dtype, max_dt)),
+                                     None if r0 is None else _ptr(r0),
+                                     None if r1 is None else _ptr(r1),
+                                     None if inf is None else _ptr(inf), _ptr(out), ctypes.byref(dt))
         if rc == 2:
             raise FloatingPointError("The calculated timestep is non-finite.")
         if rc == 3:
@@ -304,11 +312,26 @@ class OracleSWE:
         level = self.cfg.constant_level if boundary_level is None else boundary_level
         return self.o.spatial_operator(U, self.bed, self.cfg, self.dx, self.dy, level)
 
-    # src/solver.py:572-663 -> (U_new, dt as Python float)
-    def step(self, U, model_time, max_dt, boundary_level=None, infiltration=None):
+    # src/solver.py:572-663 -> (U_new, dt as Python float).  ``rainfall`` is a
+    # callable time -> rate ([1,1,ny,nx] or scalar), evaluated at the step's
+    # start (model time in the working precision) for stage 1 and half a
+    # step later for stage 2 (:607-643).
+    def step(self, U, model_time, max_dt, boundary_level=None, infiltration=None, rainfall=None):
         level = self.cfg.constant_level if boundary_level is None else boundary_level
+        rain0 = rain1 = None
+        if rainfall is not None:
+            R = self.dtype.type
+            t = float(R(model_time))
+            rain0 = rainfall(t)
+            _, ax, ay = self.o.spatial_operator(U, self.bed, self.cfg, self.dx, self.dy, level,
+                                                rain0, infiltration)
+            den = max(R(ax) / R(self.dx) + R(ay) / R(self.dy), R(self.cfg.epsilon))
+            stable = (R(1) / den) * R(self.cfg.cfl)
+            dt = stable if np.isnan(stable) else min(stable, R(max_dt))
+            if np.isfinite(dt) and dt > 0:
+                rain1 = rainfall(t + 0.5 * float(dt))
         out, dt = self.o.step(U, self.bed, self.roughness, self.cfg, self.dx, self.dy,
-                              level, max_dt, infiltration)
+                              level, max_dt, infiltration, rain0, rain1)
         return out, float(dt)
 
     # src/solver.py:680-779 -> (U, hmax, list of dt)
@@ -342,6 +365,29 @@ class OracleSWE:
                            f"requested duration={duration:.8f} s.")
 
 
+def rainfall_at(times, rates, time, dtype=np.float32):
+    """Rain rate [1,1,ny,nx] at ``time`` from records ``rates`` [nt,1,ny,nx]
+    at ``times`` [nt]: linear interpolation, held outside the series
+    (RainfallForcing.at, src/forcing.py:24-37), in ``dtype``."""
+    R = np.dtype(dtype).type
+    times = np.asarray(times, dtype=dtype)
+    rates = np.asarray(rates, dtype=dtype)
+    nt = times.size
+    if nt == 1:
+        return rates[0:1]
+    t = R(time)
+    right = min(max(int(np.searchsorted(times, t, side="left")), 1), nt - 1)
+    left = right - 1
+    width = max(times[right] - times[left], R(1.0e-12))
+    weight = (t - times[left]) / width
+    out = (R(1.0) - weight) * rates[left] + weight * rates[right]
+    if t <= times[0]:
+        out = rates[0]
+    if t >= times[-1]:
+        out = rates[-1]
+    return np.ascontiguousarray(out[None])
+
+
 def isclose_report(a, b):
     """Normwise and pointwise relative differences used by the parity tests."""
     a = np.asarray(a, dtype=np.float64)
@@ -354,4 +400,5 @@ def isclose_report(a, b):
 if os.environ.get("SWE_ORACLE_BUILD_ON_IMPORT"):
     build()
 
-__all__ = ["Oracle", "OracleSWE", "BC_CODES", "build", "lib", "num_threads", "isclose_report", "math"]
+__all__ = ["Oracle", "OracleSWE", "BC_CODES", "build", "lib", "num_threads", "isclose_report",
+           "rainfall_at", "math"]

@@ -78,7 +78,12 @@ typedef struct {
     int orc_step_##SFX(const R* U, const R* bed, int bedB, const R* n,       \
                        int nB, int B, int ny, int nx, const orc_params* p,   \
                        const R* level, R max_dt, const R* infil, R* U_out,   \
-                       R* dt_out);
+                       R* dt_out);                                           \
+    int orc_step_forced_##SFX(const R* U, const R* bed, int bedB,            \
+                              const R* n, int nB, int B, int ny, int nx,     \
+                              const orc_params* p, const R* level, R max_dt, \
+                              const R* rain0, const R* rain1,                \
+                              const R* infil, R* U_out, R* dt_out);
 
 ORC_DECLARE(float, f32)
 ORC_DECLARE(double, f64)

@@ -619,10 +619,12 @@ int FN(orc_roughness_friction)(const R* U, const R* z0, int B, int nB, int ny, i
     return 0;
 }
 
-/* SWE2D.step, src/solver.py:572-663.  level holds B values.  infil is a
- * per-cell [B,1,ny,nx] array or NULL.  *dt_out receives dt in R. */
-int FN(orc_step)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, int ny, int nx,
-                 const orc_params* p, const R* level, R max_dt, const R* infil, R* U_out, R* dt_out) {
+/* SWE2D.step, src/solver.py:572-663.  level holds B values.  rain0 / rain1
+ * (the rainfall rate of stage 1 and of stage 2, :609-643) and infil are
+ * per-cell [B,1,ny,nx] arrays or NULL.  *dt_out receives dt in R. */
+int FN(orc_step_forced)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, int ny,
+                        int nx, const orc_params* p, const R* level, R max_dt, const R* rain0,
+                        const R* rain1, const R* infil, R* U_out, R* dt_out) {
     size_t n3 = (size_t)B * 3 * ny * nx;
     R* k = (R*)malloc(sizeof(R) * n3);
     R* cand = (R*)malloc(sizeof(R) * n3);
@@ -630,7 +632,7 @@ int FN(orc_step)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, 
     int rc = 1;
     if (!k || !cand || !pred) goto done;
     R ax, ay;
-    if (FN(orc_spatial_operator)(U, bed, B, bedB, ny, nx, p, level, NULL, infil, k, &ax, &ay)) goto done;
+    if (FN(orc_spatial_operator)(U, bed, B, bedB, ny, nx, p, level, rain0, infil, k, &ax, &ay)) goto done;
     {
         /* :620-626: denominator = clamp(ax/dx + ay/dy, min=eps); cfl/den is
          * den.reciprocal() * cfl in PyTorch; dt = minimum(stable, max_dt). */
@@ -643,7 +645,7 @@ int FN(orc_step)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, 
         R hdt = (R)0.5 * dt; /* :639 */
         for (size_t i = 0; i < n3; ++i) cand[i] = U[i] + hdt * k[i];
         FN(orc_clean_and_limit)(U, cand, B, ny, nx, p, pred);
-        if (FN(orc_spatial_operator)(pred, bed, B, bedB, ny, nx, p, level, NULL, infil, k, &ax, &ay)) goto done;
+        if (FN(orc_spatial_operator)(pred, bed, B, bedB, ny, nx, p, level, rain1, infil, k, &ax, &ay)) goto done;
         for (size_t i = 0; i < n3; ++i) cand[i] = U[i] + dt * k[i]; /* :646 */
         if (p->apply_friction) {
             FN(orc_clean_and_limit)(U, cand, B, ny, nx, p, pred);
@@ -659,6 +661,13 @@ int FN(orc_step)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, 
 done:
     free(k); free(cand); free(pred);
     return rc;
+}
+
+/* The step without rainfall. */
+int FN(orc_step)(const R* U, const R* bed, int bedB, const R* n, int nB, int B, int ny, int nx,
+                 const orc_params* p, const R* level, R max_dt, const R* infil, R* U_out, R* dt_out) {
+    return FN(orc_step_forced)(U, bed, bedB, n, nB, B, ny, nx, p, level, max_dt, NULL, NULL, infil,
+                               U_out, dt_out);
 }
 
 #undef FN

@@ -1,10 +1,11 @@
 """Generate the golden fixtures of tests/golden/ from the DiffSWE2d reference.
 
-Run in a checkout where the reference source is available (default
-/root/reference); the fixtures it writes are what the tests read, so the
-reference itself never has to be present where the tests run:
+Run where the reference's source tree is available, given by --ref or the
+environment variable DIFFSWE2D_REFERENCE; the fixtures it writes are what the
+tests read, so the reference itself never has to be present where the tests
+run:
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--only ops,c1,c2,adj]
+    python tests/golden/make_golden.py --ref <reference checkout> [--only ops,c1,c2,forcing,adj]
 
 The reference is imported as the package ``diffswe2d`` from its ``src/``
 directory.  Its ``io_netcdf`` module imports ``xarray`` at load time, which
@@ -20,6 +21,9 @@ Fixtures (numpy .npz, float32 unless noted):
   adj_step.npz, adj_run.npz   reference autograd gradients (make_golden_adjoint.py)
   spline.npz      clamped B-spline basis and bounded controls of the
                   reference's inversion script
+  forcing.npz     rainfall and infiltration sources: spatial_operator with
+                  scalar / field / per-batch rates, steps with infiltration,
+                  and steps of a model forced by RainfallForcing
 """
 from __future__ import annotations
 
@@ -281,11 +285,76 @@ def make_c2(ref, out):
     np.savez_compressed(out / "c2_runup.npz", **d)
 
 
+def make_forcing(ref, out):
+    """Rainfall and infiltration (src/solver.py:437-446, :520-525, :607-643):
+    the tendency with scalar, field and per-batch rates, five steps with
+    infiltration, and five steps of a model with a RainfallForcing, all
+    with correctly-rounded sqrt/pow ("cr"), plus the stock tendency."""
+    import diffswe2d.forcing as forcing
+    rng = np.random.default_rng(4321)
+    B, ny, nx = 2, 24, 40
+    U = random_state(rng, B, ny, nx, dry_frac=0.15)
+    bed1 = random_bed(rng, 1, ny, nx)
+    n = rng.uniform(0.01, 0.04, size=(1, 1, ny, nx)).astype(np.float32)
+    rain_field = rng.uniform(0.0, 2e-3, size=(1, 1, ny, nx)).astype(np.float32)
+    rain_batch = rng.uniform(0.0, 2e-3, size=(B, 1, ny, nx)).astype(np.float32)
+    infil_field = rng.uniform(-5e-4, 1e-3, size=(1, 1, ny, nx)).astype(np.float32)
+    infil_batch = rng.uniform(-5e-4, 1e-3, size=(B, 1, ny, nx)).astype(np.float32)
+    r_times = np.array([0.0, 0.004, 0.02], np.float32)
+    r_rates = rng.uniform(0.0, 5e-3, size=(3, 1, ny, nx)).astype(np.float32)
+    d = dict(U=U, bed1=bed1, n=n, rain_field=rain_field, rain_batch=rain_batch,
+             infil_field=infil_field, infil_batch=infil_batch, r_times=r_times, r_rates=r_rates)
+    cfg = ref.SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                        boundary_bottom="transmissive", constant_level=0.2)
+    cases = {
+        "scalar": (1.5e-3, 4e-4),
+        "field": (rain_field, infil_field),
+        "batch": (rain_batch, infil_batch),
+    }
+    with torch.no_grad():
+        m = ref.SWE2D(t32(bed1[0, 0]), t32(n[0, 0]), 0.05, 0.04, config=cfg, train_dem=False)
+        for tag, (rain, infil) in cases.items():
+            r = rain if np.isscalar(rain) else t32(rain)
+            i = infil if np.isscalar(infil) else t32(infil)
+            rhs = m.spatial_operator(t32(U), rainfall_rate=r, infiltration=i, boundary_level=0.2)
+            d[f"so_{tag}"] = rhs.numpy()
+            with correctly_rounded_elementary():
+                rhs, ax, ay = m.spatial_operator(t32(U), rainfall_rate=r, infiltration=i,
+                                                 boundary_level=0.2, return_wave_speed=True)
+            d[f"socr_{tag}"] = rhs.numpy()
+            d[f"socr_{tag}_axay"] = np.array([ax, ay], np.float32)
+        for tag, infil in (("scalar", 4e-4), ("field", infil_field), ("batch", infil_batch)):
+            i = infil if np.isscalar(infil) else t32(infil)
+            Us, dts = t32(U), []
+            with correctly_rounded_elementary():
+                for _ in range(5):
+                    Us, dt = m.step(Us, 0.0, 0.05, infiltration=i, boundary_level=0.2)
+                    dts.append(dt)
+            d[f"stcr_infil_{tag}"], d[f"stcr_infil_{tag}_dts"] = Us.numpy(), np.array(dts, np.float64)
+        rf = forcing.RainfallForcing(t32(r_times), t32(r_rates))
+        mr = ref.SWE2D(t32(bed1[0, 0]), t32(n[0, 0]), 0.05, 0.04, config=cfg, train_dem=False,
+                       rainfall=rf)
+        Us, dts, t = t32(U), [], 0.0
+        with correctly_rounded_elementary():
+            for _ in range(5):
+                Us, dt = mr.step(Us, t, 0.05, infiltration=t32(infil_field), boundary_level=0.2)
+                dts.append(dt)
+                t += dt
+        d["stcr_rainfall"], d["stcr_rainfall_dts"] = Us.numpy(), np.array(dts, np.float64)
+        d["rf_at"] = np.stack([rf.at(tt).numpy() for tt in (0.0, 0.001, 0.0137, 0.5)])
+    np.savez_compressed(out / "forcing.npz", **d)
+    print("forcing.npz", len(d), "arrays")
+
+
 def main():
+    import os
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", default="ops,c1,c2")
+    ap.add_argument("--ref", default=os.environ.get("DIFFSWE2D_REFERENCE"),
+                    help="checkout of the reference (or set DIFFSWE2D_REFERENCE)")
+    ap.add_argument("--only", default="ops,c1,c2,forcing")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or DIFFSWE2D_REFERENCE")
     torch.set_num_threads(max(1, torch.get_num_threads()))
     ref = load_reference(args.ref)
     groups = set(args.only.split(","))
@@ -295,6 +364,8 @@ def main():
         make_c1(ref, HERE)
     if "c2" in groups:
         make_c2(ref, HERE)
+    if "forcing" in groups:
+        make_forcing(ref, HERE)
     if "adj" in groups:
         from make_golden_adjoint import make_adjoint  # noqa: E402
         make_adjoint(ref, HERE)

@@ -37,8 +37,29 @@ def test_binding_covers_header():
 
 def test_params_struct_layout_matches_header():
     from diffswe2d_b200 import _native
-    # 8 doubles + 8 int32 = 96 bytes, no padding
-    assert ctypes.sizeof(_native.SweParams) == 96
+    # 8 doubles + 10 int32 = 104 bytes, no padding
+    assert ctypes.sizeof(_native.SweParams) == 104
+    assert _native.SweParams.arithmetic.offset == 96
+
+
+def test_arithmetic_mode_checked():
+    """An unknown arithmetic name raises; an unknown code is rejected by the
+    library before any launch."""
+    from diffswe2d_b200 import _native as nat
+    from diffswe2d_b200.config import SWEConfig
+    with pytest.raises(ValueError):
+        nat.params(SWEConfig(), 1.0, 1.0, "approximate")
+    assert nat.params(SWEConfig(), 1.0, 1.0, "fast").arithmetic == nat.ARITH_FAST
+    p = nat.params(SWEConfig(), 1.0, 1.0)
+    p.arithmetic = 7
+    buf = ctypes.c_void_p(16)  # never dereferenced: the parameters are checked first
+    rc = nat.lib().swe_step_f32(buf, buf, 1, buf, 1, 1, 8, 8, p, buf, 1, 1.0, None, 0, 1, buf, buf,
+                                buf, None)
+    assert rc == nat.SWE_EARG
+    rc = nat.lib().swe_ensemble_run_f32(buf, 1, 0, 7, 1, 0, None)
+    assert rc == nat.SWE_EARG
+    rc = nat.lib().swe_ensemble_run_f32(buf, 1, 0, 0, 1, -1, None)
+    assert rc == nat.SWE_EARG
 
 
 def test_invalid_arguments_rejected_without_launch():

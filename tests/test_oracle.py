@@ -143,3 +143,64 @@ def test_thirty_step_loss_matches_reference(golden, fixture):
                 L = L + eta * eta
         L = L + dtype(1e-3) * (U * U).sum(dtype=dtype)
         assert float(L) == pytest.approx(float(d[key]), rel=rel)
+
+
+# ------------------------------------------------------------ rain / infiltration
+FORCING_CFG = dict(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
+                   boundary_bottom="transmissive", constant_level=0.2)
+
+
+def _forcing_case(d, tag):
+    if tag == "scalar":
+        return np.float32(1.5e-3), np.float32(4e-4)
+    if tag == "field":
+        return d["rain_field"], d["infil_field"]
+    return d["rain_batch"], d["infil_batch"]
+
+
+@pytest.mark.parametrize("tag", ["scalar", "field", "batch"])
+def test_spatial_operator_with_rain_and_infiltration(golden, o32, tag):
+    """src/solver.py:520-525: rhs[:,0] + rain - clamp(infiltration, min=0)."""
+    d = golden("forcing")
+    rain, infil = _forcing_case(d, tag)
+    rhs, ax, ay = o32.spatial_operator(d["U"], d["bed1"], SWEConfig(**FORCING_CFG), 0.05, 0.04,
+                                       0.2, rain, infil)
+    assert np.array_equal(rhs, d[f"socr_{tag}"])
+    assert np.array_equal(np.array([ax, ay], np.float32), d[f"socr_{tag}_axay"])
+    assert normwise(rhs, d[f"so_{tag}"]) < 1e-6  # stock sqrt within an ulp
+
+
+@pytest.mark.parametrize("tag", ["scalar", "field", "batch"])
+def test_steps_with_infiltration(golden, tag):
+    d = golden("forcing")
+    infil = np.float32(4e-4) if tag == "scalar" else d[f"infil_{tag}"]
+    om = OracleSWE(d["bed1"], d["n"], 0.05, 0.04, SWEConfig(**FORCING_CFG))
+    U, dts = d["U"], []
+    for _ in range(5):
+        U, dt = om.step(U, 0.0, 0.05, boundary_level=0.2, infiltration=infil)
+        dts.append(dt)
+    assert np.array_equal(U, d[f"stcr_infil_{tag}"])
+    assert np.array_equal(np.array(dts), d[f"stcr_infil_{tag}_dts"])
+
+
+def test_rainfall_interpolation_matches_reference(golden):
+    from oracle import rainfall_at
+    d = golden("forcing")
+    for k, t in enumerate((0.0, 0.001, 0.0137, 0.5)):
+        assert np.array_equal(rainfall_at(d["r_times"], d["r_rates"], t), d["rf_at"][k])
+
+
+def test_steps_with_rainfall_forcing(golden):
+    """Stage 1 at the rate of the step's start, stage 2 half a step later
+    (src/solver.py:607-643)."""
+    from oracle import rainfall_at
+    d = golden("forcing")
+    om = OracleSWE(d["bed1"], d["n"], 0.05, 0.04, SWEConfig(**FORCING_CFG))
+    U, dts, t = d["U"], [], 0.0
+    for _ in range(5):
+        U, dt = om.step(U, t, 0.05, boundary_level=0.2, infiltration=d["infil_field"],
+                        rainfall=lambda tt: rainfall_at(d["r_times"], d["r_rates"], tt))
+        dts.append(dt)
+        t += dt
+    assert np.array_equal(U, d["stcr_rainfall"])
+    assert np.array_equal(np.array(dts), d["stcr_rainfall_dts"])
