@@ -6,22 +6,30 @@ friction included) and its fraction of the HBM roofline.
 
 Workload: the runup scenario (plane beach + 20 seeded Gaussian bumps, west
 water-level inflow from a leading-depression N-wave, walls elsewhere,
-Manning n = 0.01, dx = 0.014 m) tiled to 4096 x 4096 cells; synthetic data.
+Manning n = 0.01, dx = 0.014 m) after 8 s of simulated time (waves and
+wet/dry fronts), tiled to 4096 x 4096 cells; synthetic data.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--arithmetic fast|exact]
 
 One process per GPU (torchrun for N > 1).  Each rank steps its own replica of
 the grid -- the single-grid step has no exchange (weak scaling) -- and rank 0
 prints one JSON line.  ``value`` is device-timed with CUDA events around K
-steps with inputs resident in HBM; ``e2e`` is the same metric through the
-public ``SWE2D.forward`` call with the state copied from pinned host memory
-and back inside the timed region.  ``--impl reference`` times the CPU oracle
-(a C restatement of the reference step, all host threads) on a bounded crop
-of the same workload.
+steps of the tolerance-mode kernels (``--arithmetic``; the IEEE kernels are
+timed too and reported under ``exact_arithmetic``) with inputs resident in
+HBM; ``e2e`` is the same metric through the public ``SWE2D.forward`` call
+with the state copied from pinned host memory and back inside the timed
+region.  Outside the timed regions: ``parity`` (three steps of a crop, IEEE
+kernels bit for bit against the CPU oracle, tolerance mode's error),
+``cpu_baseline`` and ``reference_torch`` (the reference's own PyTorch step,
+eager on the host cores and eager / compiled on the GPU).
+``--impl reference`` times the CPU oracle (a C restatement of the reference
+step, all host threads) on a bounded crop of the same workload.
 """
 from __future__ import annotations
 
 import argparse
+import contextlib
 import ctypes
 import json
 import os
@@ -38,12 +46,17 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 BYTES_PER_CELL_UPDATE = 32  # read h,hu,hv,z,n once, write h,hu,hv once
-# DRAM bytes per cell of one stage-2 launch from the ncu capture of
-# profiles/sweep_kernels_runup_3072.md (302.1 MB read + 95.9 MB written over
-# 3072^2 cells); traffic grows with the cells, so a launch of the bench's grid
-# moves this many bytes per cell.
-STAGE2_DRAM_BYTES_PER_CELL = (302.098944e6 + 95.926016e6) / (3072 * 3072)
 STAGE2_BYTES_PER_CELL = 44  # stage-2 kernel: read U, k1, z, n; write U
+# DRAM bytes per cell of one stage-2 launch, from ncu captures of the same
+# kernel on a smaller grid of the same workload (traffic grows with the
+# cells, so a launch of the bench's grid moves this many bytes per cell).
+STAGE2_DRAM_BYTES_PER_CELL = {
+    # IEEE kernels: 302.1 MB read + 95.9 MB written over 3072^2 cells
+    "exact": (302.098944e6 + 95.926016e6) / (3072 * 3072),
+}
+STAGE2_TRAFFIC_SOURCE = {
+    "exact": "ncu dram__bytes_read+write of the IEEE stage-2 kernel at 3072^2, scaled by cells",
+}
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -53,11 +66,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--arithmetic", choices=["exact", "fast"], default="exact")
+    ap.add_argument("--arithmetic", choices=["exact", "fast"], default="fast",
+                    help="step kernels of the headline number (the other mode is reported too)")
     ap.add_argument("--ny", type=int, default=4096)
     ap.add_argument("--nx", type=int, default=4096)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU oracle timing and the parity check on a crop")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-context", action="store_true",
+                    help="skip timing the reference's own PyTorch step (baseline/_ref)")
+    ap.add_argument("--reference-context", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["runup4096", "ensemble", "inversion", "warmstart"],
                     default="runup4096",
                     help="runup4096: the headline single-grid step; ensemble: 64 scenarios of "
@@ -79,6 +97,10 @@ def parse():
     return ap.parse_args()
 
 
+def world_size() -> int:
+    return int(os.environ.get("WORLD_SIZE", "1"))
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -95,8 +117,7 @@ def dist_setup(args):
 
 def workload(ny, nx):
     from diffswe2d_b200 import scenarios
-    base = scenarios.runup(seed=0)
-    return scenarios.tiled(base, ny, nx)
+    return scenarios.throughput_workload(ny, nx)
 
 
 def level_at(sc, t: float) -> float:
@@ -109,55 +130,59 @@ def level_at(sc, t: float) -> float:
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clock and clock-event (throttle) reasons sampled every few
+    milliseconds through NVML while a region runs (read only; nothing is
+    changed)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+    def __init__(self, index: int, period_s: float = 0.005):
+        self.index, self.period = index, period_s
+        self.samples, self.max_mhz, self.reasons = [], None, set()
+        self.error = None
+
+    def _poll(self):
+        try:
+            import pynvml
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            while not self._stop.is_set():
+                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, bit in self.REASONS.items():
+                    if bits & bit:
+                        self.reasons.add(name)
+                self._stop.wait(self.period)
+        except Exception as e:  # sampling must never break the measurement
+            self.error = repr(e)
 
     def __enter__(self):
+        import threading
+        self._stop = threading.Event()
+        self._thread = None
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.index)],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+        except Exception as e:
+            self.error = repr(e)
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
         return False
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in getattr(self, "lines", []):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+               "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+               "samples": len(self.samples), "source": "NVML, every 5 ms during the timed region"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def measured_peaks():
@@ -168,31 +193,322 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def crop_of(sc, crop):
+    """The top-left crop x crop block of a scenario as a scenario of its own
+    (same configuration: west water level, walls elsewhere)."""
+    from diffswe2d_b200.scenarios import Scenario
+    return Scenario(f"{sc.name}_crop{crop}", np.ascontiguousarray(sc.bed[:crop, :crop]),
+                    np.ascontiguousarray(sc.roughness[:crop, :crop]),
+                    np.ascontiguousarray(sc.U0[:, :, :crop, :crop]), sc.dx, sc.dy, dict(sc.config),
+                    sc.bc_times, sc.bc_levels, sc.steps, dict(sc.meta))
+
+
 def cpu_baseline(sc, max_seconds=12.0, crop=1024):
-    """The CPU oracle (C restatement, all host threads) on a crop of the workload."""
+    """The CPU oracle (C restatement of the reference step, all host threads)
+    on a crop of the workload."""
     sys.path.insert(0, str(REPO / "oracle"))
     from oracle import OracleSWE, num_threads
     from diffswe2d_b200.config import SWEConfig
-    bed = sc.bed[:crop, :crop]
-    m = OracleSWE(bed, sc.roughness[:crop, :crop], sc.dx, sc.dy, SWEConfig(**sc.config))
-    U = np.ascontiguousarray(sc.U0[:, :, :crop, :crop])
-    U, _ = m.step(U, 0.0, 1.0e9, boundary_level=level_at(sc, 0.0))  # warm caches
-    steps, t0, t = 0, time.perf_counter(), 0.0
+    c = crop_of(sc, crop)
+    m = OracleSWE(c.bed, c.roughness, c.dx, c.dy, SWEConfig(**c.config))
+    t = c.meta.get("start_time", 0.0)
+    U, dt = m.step(c.U0, t, 1.0e9, boundary_level=level_at(c, t))  # warm caches
+    t += dt
+    steps, t0 = 0, time.perf_counter()
     while True:
-        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(c, t))
         t += dt
         steps += 1
         el = time.perf_counter() - t0
         if el > max_seconds or steps >= 200:
             break
-    cells = bed.size
+    cells = c.bed.size
     return {"value": cells * steps / el / 1e6, "unit": "Mcell-updates/s", "cores": num_threads(),
             "kind": "port",
             "sample": f"{steps} steps of a {crop}x{crop} crop of the workload ({el:.1f} s)"}
 
 
+def parity_on_crop(sc, dev, crop=1024, steps=3):
+    """Outside the timed region: `steps` steps of a crop of the workload by
+    the IEEE kernels (bit for bit against the CPU oracle) and by the
+    tolerance-mode kernels (normwise error against the oracle, wet/dry
+    mask), through SWE2D.step."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import OracleSWE
+    from diffswe2d_b200 import SWE2D, SWEConfig
+    c = crop_of(sc, crop)
+    cfg = SWEConfig(**c.config)
+    om = OracleSWE(c.bed, c.roughness, c.dx, c.dy, cfg)
+    t0 = c.meta.get("start_time", 0.0)
+    U, t, ref, dts = c.U0, t0, [], []
+    for _ in range(steps):
+        U, dt = om.step(U, t, 1.0e9, boundary_level=level_at(c, t))
+        t += dt
+        ref.append(U)
+        dts.append(dt)
+    out = {"crop": [crop, crop], "steps": steps}
+    for mode in ("exact", "fast"):
+        m = SWE2D(torch.from_numpy(c.bed).to(dev), torch.from_numpy(c.roughness).to(dev), c.dx, c.dy,
+                  config=cfg, train_dem=False, arithmetic=mode)
+        Ug, t, same_dt = torch.from_numpy(c.U0).to(dev), t0, True
+        with torch.no_grad():
+            for k in range(steps):
+                Ug, dt = m.step(Ug, t, 1.0e9, boundary_level=level_at(c, t))
+                same_dt &= dt == dts[k]
+                t += dt
+        Uh = Ug.cpu().numpy()
+        if mode == "exact":
+            out["exact_bitwise_vs_oracle"] = bool(np.array_equal(Uh.view(np.uint32),
+                                                                 ref[-1].view(np.uint32)) and same_dt)
+        else:
+            errs = []
+            for ch in range(3):
+                a, b = Uh[:, ch].astype(np.float64), ref[-1][:, ch].astype(np.float64)
+                errs.append(float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)))
+            out["fast_normwise_vs_oracle"] = errs
+            out["fast_wet_mask_equal"] = bool(np.array_equal(Uh[:, 0] > 1e-6, ref[-1][:, 0] > 1e-6))
+    return out
+
+
+def time_single_grid(sc, args, dev, arithmetic, clocks=None):
+    """K device-timed steps of the single-grid step (the two stage kernels
+    enqueued through the C ABI, a CUDA event after each) on the workload,
+    after W untimed ones; inputs resident in HBM and larger than L2."""
+    from diffswe2d_b200 import SWEConfig, autotune
+    from diffswe2d_b200 import _native as nat
+    ny, nx = sc.bed.shape
+    cells = ny * nx
+    cfg = SWEConfig(**sc.config)
+    tuning = autotune.tune(dev, arithmetic=arithmetic)
+    rows = autotune.tuned_rows(cells, dev, arithmetic)
+    lib = nat.lib()
+    nat.check(lib.swe_tune_sweep_rows(rows), "tuned rows")
+    p = nat.params(cfg, sc.dx, sc.dy, arithmetic)
+    bed = torch.from_numpy(sc.bed).to(dev)
+    n = torch.from_numpy(sc.roughness).to(dev)
+    U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]
+    k1 = torch.empty_like(U[0])
+    red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
+    stream = nat.stream_handle(dev)
+    total = args.warmup + args.steps
+    lev = torch.zeros(total, dtype=torch.float32, device=dev)
+
+    def launch(i, src, dst, stage):
+        rc = lib.swe_step_stage_f32(stage, nat.ptr(src), nat.ptr(bed), 1, nat.ptr(n), 1, 1, ny, nx, p,
+                                    ctypes.c_void_p(lev.data_ptr() + 4 * i), 1, 1.0e9, None, 0, 1,
+                                    nat.ptr(k1), nat.ptr(red), nat.ptr(dst), stream)
+        nat.check(rc, "step")
+
+    # Host-side replica of the model time so every step sees the inflow level
+    # of its own time, staged on the device before the timed region: the CFL
+    # step barely changes over a few hundred steps, one probe step fixes it.
+    t = sc.meta.get("start_time", 0.0)
+    lev.fill_(level_at(sc, t))
+    launch(0, U[0], U[1], 3)
+    dt_probe = float(red[3:4].view(torch.float32).item())
+    lev.copy_(torch.tensor([level_at(sc, t + i * dt_probe) for i in range(total)], dtype=torch.float32))
+    src = 0
+    for i in range(args.warmup):
+        launch(i, U[src], U[1 - src], 3)
+        src = 1 - src
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    if world_size() > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with clocks if clocks is not None else contextlib.nullcontext():
+        ev[0].record()
+        for k in range(args.steps):
+            i = args.warmup + k
+            launch(i, U[src], U[1 - src], 1)
+            ev[2 * k + 1].record()
+            launch(i, U[src], U[1 - src], 2)
+            ev[2 * k + 2].record()
+            src = 1 - src
+        torch.cuda.synchronize(dev)
+    total_ms = ev[0].elapsed_time(ev[-1])
+    s1 = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+    s2 = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)]
+    return {"total_ms": total_ms, "stage1_ms": statistics.mean(s1), "stage2_ms": statistics.mean(s2),
+            "rows": rows,
+            "tuned_rows": tuning.get("rows" if arithmetic == "exact" else f"rows_{arithmetic}"),
+            "status": int(red[2].item()), "finite": bool(torch.isfinite(U[src]).all().item()),
+            "dt_probe": dt_probe}
+
+
+def end_to_end(sc, args, dev, world, arithmetic, dt_probe):
+    """The same metric through the public API: each call is SWE2D.forward(U0,
+    t_end = about 100 CFL steps) on the state copied in from pinned host
+    memory, with the result copied back to pinned host memory, inside the
+    timed region."""
+    from diffswe2d_b200 import SWE2D, SWEConfig
+    from diffswe2d_b200.sharding import reduce_over_ranks
+    ny, nx = sc.bed.shape
+    model = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev),
+                  sc.dx, sc.dy, config=SWEConfig(**sc.config), train_dem=False, arithmetic=arithmetic)
+    model.set_dynamic_boundary(torch.from_numpy(sc.bc_times).to(dev),
+                               torch.from_numpy(sc.bc_levels).to(dev))
+    t0 = sc.meta.get("start_time", 0.0)
+    host_in = torch.from_numpy(sc.U0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    span = 100 * dt_probe
+    for _ in range(2):  # warm-up (captures the device loop's graph)
+        Uf, _ = model(host_in.to(dev, non_blocking=True), t_end=span, start_time=t0)
+        host_out.copy_(Uf, non_blocking=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    calls, counts = 3, []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(calls):
+        Uf, _ = model(host_in.to(dev, non_blocking=True), t_end=span, start_time=t0)
+        host_out.copy_(Uf, non_blocking=True)
+        counts.append(model.last_forward_steps)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = reduce_over_ranks([e0.elapsed_time(e1)], "max", dev)[0]
+    nbytes = host_in.numel() * 4
+    steps = sum(counts)
+    return {"value": world * ny * nx * steps / (ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+            "h2d_bytes_per_step": nbytes * calls / steps, "d2h_bytes_per_step": nbytes * calls / steps,
+            "h2d_bytes_per_call": nbytes, "d2h_bytes_per_call": nbytes,
+            "internal_steps_per_call": counts,
+            "api": "SWE2D.forward(U0 from pinned host, t_end = about 100 CFL steps; device-driven "
+                   "time loop) + state back to pinned host, per call; bytes per step are the "
+                   "per-call copies divided by the solver steps of the call"}
+
+
+REFERENCE_TARGET = REPO / "baseline" / "_ref"
+
+
+def reference_context(args, timeout_s=420):
+    """The reference's own PyTorch step (installed into baseline/_ref), timed
+    in a child process outside every timed region of this run: eager on the
+    host cores (a crop), eager on the GPU and torch.compile'd on the GPU
+    (the full grid).  Context for the kernels' numbers, not a bench line."""
+    if not (REFERENCE_TARGET / "diffswe2d" / "solver.py").exists():
+        return {"unavailable": "the reference is not installed in baseline/_ref"}
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--reference-context",
+           "--ny", str(args.ny), "--nx", str(args.nx)]
+    note = None
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+        stdout, stderr = out.stdout, out.stderr
+    except subprocess.TimeoutExpired as e:
+        stdout = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
+        stderr = ""
+        note = f"stopped after {timeout_s} s"
+    for line in reversed(stdout.splitlines()):
+        if line.startswith("{"):
+            res = json.loads(line)
+            if note:
+                res["note"] = note
+            elif "cuda_compile" not in res and stderr.strip():
+                res["note"] = "stopped: " + stderr.strip().splitlines()[-1]
+            return res
+    return {"unavailable": note or ("reference timing failed: "
+                                    + (stderr.strip().splitlines() or ["?"])[-1])}
+
+
+def _import_reference():
+    import importlib.machinery
+    import types
+    if "xarray" not in sys.modules:
+        try:
+            import xarray  # noqa: F401
+        except ImportError:  # only the reference's NetCDF reader needs it
+            stub = types.ModuleType("xarray")
+            stub.__spec__ = importlib.machinery.ModuleSpec("xarray", None)
+            sys.modules["xarray"] = stub
+    sys.path.insert(0, str(REFERENCE_TARGET))
+    import diffswe2d
+    return diffswe2d
+
+
+def run_reference_context(args):
+    """Child process of reference_context: prints one JSON object."""
+    ref = _import_reference()
+    sc = workload(args.ny, args.nx)
+    t0 = sc.meta.get("start_time", 0.0)
+    res = {"code": "reference SWE2D (baseline/_ref, unmodified), float32"}
+
+    def model_on(dev, c):
+        m = ref.SWE2D(torch.from_numpy(c.bed).to(dev), torch.from_numpy(c.roughness).to(dev), c.dx, c.dy,
+                      config=ref.SWEConfig(**c.config), train_dem=False)
+        m.set_dynamic_boundary(torch.from_numpy(c.bc_times).to(dev), torch.from_numpy(c.bc_levels).to(dev))
+        return m
+
+    # eager, host cores, on a crop
+    crop = 512
+    c = crop_of(sc, crop)
+    torch.set_num_threads(os.cpu_count() or 1)
+    m = model_on("cpu", c)
+    U, t = torch.from_numpy(c.U0), t0
+    with torch.no_grad():
+        U, dt = m.step(U, t, 1.0e9, boundary_level=m._interpolate_dynamic_boundary(t, U))
+        t += dt
+        steps, start = 0, time.perf_counter()
+        while time.perf_counter() - start < 8.0 and steps < 50:
+            U, dt = m.step(U, t, 1.0e9, boundary_level=m._interpolate_dynamic_boundary(t, U))
+            t += dt
+            steps += 1
+        el = time.perf_counter() - start
+    res["cpu_eager"] = {"value": crop * crop * steps / el / 1e6, "unit": "Mcell-updates/s",
+                        "threads": torch.get_num_threads(), "sample": f"{steps} steps, {crop}x{crop} crop"}
+    print(json.dumps(res), flush=True)
+    if not torch.cuda.is_available():
+        return
+    dev = torch.device("cuda", 0)
+    ny, nx = sc.bed.shape
+    m = model_on(dev, sc)
+    U0 = torch.from_numpy(sc.U0).to(dev)
+
+    def timed(fn, count):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        steps = fn(count)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return ny * nx * steps / (e0.elapsed_time(e1) * 1e-3) / 1e6
+
+    def eager(count):
+        U, t = U0, t0
+        with torch.no_grad():
+            for _ in range(count):
+                U, dt = m.step(U, t, 1.0e9, boundary_level=m._interpolate_dynamic_boundary(t, U))
+                t += dt
+        return count
+
+    eager(2)
+    res["cuda_eager"] = {"value": timed(eager, 10), "unit": "Mcell-updates/s",
+                         "sample": f"10 steps of the {ny}x{nx} grid"}
+    print(json.dumps(res), flush=True)
+    # the reference's own usage: torch.compile(model) around forward()
+    cm = torch.compile(m)
+    dt0 = float(m.stable_dt(U0, boundary_level=m._interpolate_dynamic_boundary(t0, U0)))
+    start = time.perf_counter()
+    counted = []
+
+    def compiled(count):
+        counted.clear()
+        with torch.no_grad():
+            cm(U0, t_end=count * dt0, start_time=t0, callback=lambda i, t, U: counted.append(i))
+        return len(counted)
+
+    compiled(3)
+    res["cuda_compile_seconds"] = time.perf_counter() - start
+    res["cuda_compile"] = {"value": timed(compiled, 10), "unit": "Mcell-updates/s",
+                           "sample": f"forward() of about 10 steps of the {ny}x{nx} grid, "
+                                     "torch.compile(model) as the reference's examples do"}
+    print(json.dumps(res), flush=True)
+
+
 def run_reference(args, world, rank):
-    """--impl reference: the CPU oracle port of the reference step, rank 0 only."""
+    """--impl reference: the CPU oracle port of the reference step (all host
+    threads), rank 0 only, on a 1024x1024 crop of the workload."""
     if rank != 0:
         return
     sc = workload(args.ny, args.nx)
@@ -200,16 +516,15 @@ def run_reference(args, world, rank):
     from oracle import OracleSWE, num_threads
     from diffswe2d_b200.config import SWEConfig
     crop = 1024
-    m = OracleSWE(sc.bed[:crop, :crop], sc.roughness[:crop, :crop], sc.dx, sc.dy,
-                  SWEConfig(**sc.config))
-    U = np.ascontiguousarray(sc.U0[:, :, :crop, :crop])
-    t = 0.0
+    c = crop_of(sc, crop)
+    m = OracleSWE(c.bed, c.roughness, c.dx, c.dy, SWEConfig(**c.config))
+    U, t = c.U0, c.meta.get("start_time", 0.0)
     for _ in range(args.warmup):
-        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(c, t))
         t += dt
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(sc, t))
+        U, dt = m.step(U, t, 1.0e9, boundary_level=level_at(c, t))
         t += dt
     el = time.perf_counter() - t0
     value = crop * crop * args.steps / el / 1e6
@@ -438,6 +753,9 @@ def run_warmstart(args, world, rank, local):
 
 def main():
     args = parse()
+    if args.reference_context:
+        run_reference_context(args)
+        return
     world, rank, local = dist_setup(args)
     if args.workload == "ensemble" and args.impl == "b200":
         run_ensemble(args, world, rank, local)
@@ -466,152 +784,85 @@ def main():
     sc = workload(args.ny, args.nx)
     ny, nx = sc.bed.shape
     cells = ny * nx
-    cfg = SWEConfig(**sc.config)
-    # launch shape from the project's autotuner (sweep tile rows per size class)
-    from diffswe2d_b200 import autotune
-    tuning = autotune.tune(dev, arithmetic=args.arithmetic)
-    autotune.apply(dev, cells, args.arithmetic)
-    rows_used = autotune.tuned_rows(cells, dev, args.arithmetic)
-    model = SWE2D(torch.from_numpy(sc.bed).to(dev), torch.from_numpy(sc.roughness).to(dev),
-                  sc.dx, sc.dy, config=cfg, train_dem=False, arithmetic=args.arithmetic)
-    model.set_dynamic_boundary(torch.from_numpy(sc.bc_times).to(dev),
-                               torch.from_numpy(sc.bc_levels).to(dev))
-    lib = nat.lib()
-    p = nat.params(cfg, sc.dx, sc.dy, args.arithmetic)
-    bed = model.bed.detach().contiguous()
-    n = model.roughness_length.contiguous()
-    U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]
-    k1 = torch.empty_like(U[0])
-    red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=dev)
-    stream = nat.stream_handle(dev)
-    # Host-side replica of the model time so every step sees the inflow level of
-    # its own time; the levels are staged on the device before the timed region.
-    total = args.warmup + args.steps
-    levels_host, t = [], 0.0
-    dt_probe = None
-    lev = torch.zeros(total, dtype=torch.float32, device=dev)
-
-    def launch(i, src, dst, stage):
-        rc = lib.swe_step_stage_f32(stage, nat.ptr(src), nat.ptr(bed), 1, nat.ptr(n), 1, 1, ny, nx, p,
-                                    ctypes.c_void_p(lev.data_ptr() + 4 * i), 1, 1.0e9, None, 0, 1,
-                                    nat.ptr(k1), nat.ptr(red), nat.ptr(dst), stream)
-        nat.check(rc, "step")
-
-    # The CFL time step of this workload barely changes over a few hundred
-    # steps; one probe step fixes the schedule of inflow levels.
-    launch(0, U[0], U[1], 3)
-    dt_probe = float(red[3:4].view(torch.float32).item())
-    for i in range(total):
-        levels_host.append(level_at(sc, t))
-        t += dt_probe
-    lev.copy_(torch.tensor(levels_host, dtype=torch.float32))
-
-    src = 0
-    for i in range(args.warmup):
-        launch(i, U[src], U[1 - src], 3)
-        src = 1 - src
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    with Clocks(local) as clk:
-        ev[0].record()
-        for k in range(args.steps):
-            i = args.warmup + k
-            launch(i, U[src], U[1 - src], 1)
-            ev[2 * k + 1].record()
-            launch(i, U[src], U[1 - src], 2)
-            ev[2 * k + 2].record()
-            src = 1 - src
-        torch.cuda.synchronize(dev)
-    total_ms = ev[0].elapsed_time(ev[-1])
-    s1 = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
-    s2 = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)]
+    modes = [args.arithmetic] + [m for m in ("fast", "exact") if m != args.arithmetic]
+    runs, clk = {}, None
+    for mode in modes:
+        c = Clocks(local)
+        runs[mode] = time_single_grid(sc, args, dev, mode, c)
+        if mode == args.arithmetic:
+            clk = c
+    head = runs[args.arithmetic]
     from diffswe2d_b200.sharding import reduce_over_ranks
-    total_ms = reduce_over_ranks([total_ms], "max", dev)[0]  # max over ranks
-    ms_per_step = total_ms / args.steps
-    value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
-    status = int(red[2].item())
-    finite = bool(torch.isfinite(U[src]).all().item())
+    for r in runs.values():
+        r["total_ms"] = reduce_over_ranks([r["total_ms"]], "max", dev)[0]  # max over ranks
+        r["value"] = world * cells * args.steps / (r["total_ms"] * 1e-3) / 1e6
+        r["ms_per_step"] = r["total_ms"] / args.steps
 
-    # End to end: SWE2D.forward through the public API with the state copied
-    # in from pinned host memory and back out every step.
     e2e = None
     if not args.no_e2e:
-        host_in = torch.from_numpy(sc.U0).pin_memory()
-        host_out = torch.empty_like(host_in).pin_memory()
-        chunk = 20 * dt_probe  # about 20 internal CFL steps per call
-        counts = []
-        e2e_steps = 3
-        for w in range(2):  # warm-up
-            Ud = host_in.to(dev, non_blocking=True)
-            Uf, _ = model(Ud, t_end=chunk, start_time=0.0)
-            host_out.copy_(Uf, non_blocking=True)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for s in range(e2e_steps):
-            Ud = host_in.to(dev, non_blocking=True)
-            Uf, _ = model(Ud, t_end=chunk, start_time=0.0)
-            host_out.copy_(Uf, non_blocking=True)
-            counts.append(model.last_forward_steps)
-        e1.record()
-        torch.cuda.synchronize(dev)
-        e2e_ms = reduce_over_ranks([e0.elapsed_time(e1)], "max", dev)[0]
-        nbytes = host_in.numel() * 4
-        e2e = {"value": world * cells * sum(counts) / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "api": "SWE2D.forward(U0 from pinned host, t_end=~20 CFL steps; device-driven "
-                      "time loop) + state back to host",
-               "internal_steps_per_call": counts}
+        e2e = end_to_end(sc, args, dev, world, args.arithmetic, head["dt_probe"])
 
     peak, peak_kind = measured_peaks()
-    s2_avg = statistics.mean(s2)
-    s1_avg = statistics.mean(s1)
-    achieved = STAGE2_BYTES_PER_CELL * cells / (s2_avg * 1e-3) / 1e9
-    step_achieved = BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
+
+    def roofline(r, mode):
+        achieved = STAGE2_BYTES_PER_CELL * cells / (r["stage2_ms"] * 1e-3) / 1e9
+        step_achieved = BYTES_PER_CELL_UPDATE * cells / (r["ms_per_step"] * 1e-3) / 1e9
+        traffic = STAGE2_DRAM_BYTES_PER_CELL.get(mode)
+        return {"bound": "hbm", "kernel": f"stage 2 ({mode} arithmetic): predictor + tendency + "
+                                          "corrector + friction",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None if traffic is None else traffic * cells,
+                "traffic_source": STAGE2_TRAFFIC_SOURCE.get(mode),
+                "peak_kind": peak_kind, "bytes_per_cell": STAGE2_BYTES_PER_CELL,
+                "stage1_ms": r["stage1_ms"], "stage2_ms": r["stage2_ms"],
+                "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak,
+                "step_bytes_per_cell_update": BYTES_PER_CELL_UPDATE}
+
     line = {
         "metric": "Mcell-updates/s & %HBM peak",
-        "value": value,
+        "value": head["value"],
         "unit": "Mcell-updates/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
+        "ms_per_step": head["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"runup_tiled_{ny}x{nx}", "grid": [ny, nx], "dx": sc.dx,
+                   "state": f"runup scenario after {sc.meta.get('start_time', 0.0):g} s of simulated "
+                            "time (waves, wet/dry fronts), tiled",
                    "boundaries": "west water_level (N-wave), walls", "manning": 0.01,
+                   "arithmetic": args.arithmetic,
                    "l2": "inputs larger than L2: state 201 MB + k1 201 MB + bed/n 134 MB per replica",
-                   "parallelism": f"replicas x{world}", "sweep_tile_rows": rows_used,
-                   "tuned_rows_by_size_class": tuning.get("rows")},
-        "roofline": {"bound": "hbm", "kernel": "stage2 (predictor+tendency+corrector+friction)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": STAGE2_DRAM_BYTES_PER_CELL * cells,
-                     "traffic_source": "ncu dram__bytes_read+write of stage 2 at 3072^2, scaled by cells",
-                     "peak_kind": peak_kind,
-                     "bytes_per_cell": STAGE2_BYTES_PER_CELL,
-                     "stage1_ms": s1_avg, "stage2_ms": s2_avg,
-                     "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak,
-                     "step_bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+                   "parallelism": f"replicas x{world}", "sweep_tile_rows": head["rows"],
+                   "tuned_rows_by_size_class": head["tuned_rows"]},
+        "roofline": roofline(head, args.arithmetic),
         "gpu_launches": 2 * args.steps,
-        "clocks": clk.summary(),
-        "status_word": status,
-        "state_finite": finite,
+        "clocks": clk.summary() if clk is not None else None,
+        "status_word": head["status"],
+        "state_finite": head["finite"],
     }
+    for mode, r in runs.items():
+        if mode != args.arithmetic:
+            line[f"{mode}_arithmetic"] = {"value": r["value"], "unit": "Mcell-updates/s",
+                                          "ms_per_step": r["ms_per_step"],
+                                          "sweep_tile_rows": r["rows"],
+                                          "roofline": roofline(r, mode),
+                                          "status_word": r["status"], "state_finite": r["finite"]}
     if e2e is not None:
         line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc)
+        line["parity"] = parity_on_crop(sc, dev)
+    if rank == 0 and world == 1 and not args.no_reference_context:
+        line["reference_torch"] = reference_context(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
 

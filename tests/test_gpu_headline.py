@@ -1,5 +1,5 @@
-"""Parity on the throughput workload itself: the 244x393 runup scenario spun
-up for 8 s of simulated time (waves and wet/dry fronts), tiled to 4096x4096
+"""Parity on the throughput workload itself: the 244x393 runup scenario after
+8 s of simulated time (waves and wet/dry fronts), tiled to 4096x4096
 (16.8 M cells, state and inputs larger than L2), at the tile height the
 autotuner picks for that size -- the launch that bench.py times.
 
@@ -27,7 +27,7 @@ STEPS = 3
 def workload():
     autotune.tune(DEV)  # the tile heights bench.py uses (cached per device)
     autotune.tune(DEV, arithmetic="fast")
-    sc = scenarios.throughput_workload(4096, 4096, DEV)
+    sc = scenarios.throughput_workload(4096, 4096)
     cfg = SWEConfig(**sc.config)
     t0 = sc.meta["start_time"]
     om = OracleSWE(sc.bed, sc.roughness, sc.dx, sc.dy, cfg)
@@ -58,6 +58,15 @@ def _gpu_steps(sc, cfg, arithmetic, rows):
     finally:
         nat.check(lib.swe_tune_sweep_rows(prev), "rows")
     return out
+
+
+def test_stored_spun_up_state_is_what_the_kernels_compute():
+    """The workload's stored initial state (the runup scenario at 8 s,
+    computed on the CPU) equals SWE2D.forward's IEEE kernels run for 8 s
+    from the scenario's initial state, bit for bit."""
+    sc = scenarios.spun_up(scenarios.runup(seed=0), scenarios.WORKLOAD_SPIN_UP_S, DEV)
+    stored = scenarios.runup_at_spin_up()
+    assert np.array_equal(sc.U0.view(np.uint32), stored.U0.view(np.uint32))
 
 
 def test_workload_is_not_at_rest(workload):
