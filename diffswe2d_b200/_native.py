@@ -21,6 +21,7 @@ ARITHMETIC = {"exact": ARITH_EXACT, "fast": ARITH_FAST}
 S_NONFINITE_STATE, S_NONFINITE_DT, S_NONPOSITIVE_DT, S_STEP_LIMIT = 1, 2, 4, 8
 RED_WORDS = 8
 FORCING_NONE, FORCING_SCALAR, FORCING_FIELD = 0, 1, 2
+NN_GEMM_WAIT_NS = 1_000_000_000  # nn_gemm_bf16's normal wait limit (include/nn_b200.h)
 
 BC_CODES = {
     "transmissive": 0,
@@ -185,7 +186,8 @@ _SIGNATURES = {
     "swe_sweep_rows": [],
     "swe_load_kernels": [],
     # include/nn_b200.h
-    "nn_gemm_bf16": [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P],
+    "nn_gemm_bf16": [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, ctypes.c_longlong,
+                     _P, _P],
     "nn_im2col": [_P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _F, _P, _I, _P],
     "nn_col2im": [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P],
     "nn_act_backward": [_P, _P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _P],

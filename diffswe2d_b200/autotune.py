@@ -11,7 +11,11 @@ Two knobs are tuned by timing them on the GPU in use:
   ``SWE2D.forward`` (``tuned_rows_for_shape``);
 * the number of steps per CUDA-graph replay of ``SWE2D.forward``'s device
   loop -- more steps per replay mean fewer host reads, more no-op steps at
-  the end of a call.
+  the end of a call;
+* the checkpoint interval k of a differentiated gauge run
+  (``tuned_checkpoint_every``) -- memory O(steps/k + k) states; a longer k
+  means fewer checkpoints but a longer recomputed (or copied) segment held
+  at once and longer captured graphs -- timed on the run itself.
 
 Tile heights are tuned separately for the two arithmetic modes of the step
 kernels ("exact" and "fast"), whose register use and cost per cell differ.
@@ -237,6 +241,75 @@ def tuned_rows_for_shape(batch: int, ny: int, nx: int, device="cuda", steps: int
     return int(best)
 
 
+CHECKPOINT_CHOICES = (32, 64, 128, 256)
+
+
+def tuned_checkpoint_every(model, U0, levels, out_dt: float, gauges, max_dt_cap=None,
+                           store_states=None, budget_frac: float = 0.25, force: bool = False) -> int:
+    """Checkpoint interval k of ``gauge_run`` for this model, state shape,
+    interval count and storage mode: the k in CHECKPOINT_CHOICES whose
+    forward + backward gauge run is fastest, timed on the first intervals of
+    the caller's own run (about 1500 solver steps), among the k whose
+    segment and checkpoint buffers fit in ``budget_frac`` of the free device
+    memory.  Cached per device like the tile heights."""
+    from .gauge_run import CHECKPOINT_EVERY, GRAPH_STEPS, gauge_run
+    dev = U0.device
+    B, _, ny, nx = U0.shape
+    lv = levels.detach()
+    n_out = lv.shape[-1]
+    entry = _load(dev)
+    key = (f"{model.arithmetic}/{B}x{ny}x{nx}/{n_out}x{float(out_dt):.6g}/"
+           f"{len(gauges)}g/{'store' if store_states else 'auto' if store_states is None else 'recompute'}")
+    table = entry.setdefault("checkpoint_every", {})
+    if key in table and not force:
+        return int(table[key]["k"])
+    Ud = U0.detach()
+    # steps per interval, from one forward pass of a few intervals
+    probe = lv[..., : min(n_out, 4)]
+    with torch.no_grad():
+        gauge_run(model, Ud, probe, out_dt, gauges, max_dt_cap=max_dt_cap,
+                  checkpoint_every=CHECKPOINT_EVERY, store_states=False)
+    from .gauge_run import _WORKSPACES
+    per_interval = max(1, list(_WORKSPACES.values())[0].last_steps // probe.shape[-1])
+    n_t = max(1, min(n_out, -(-1536 // per_interval)))
+    lv_t = lv[..., :n_t].contiguous()
+    state_bytes = 4 * 3 * B * ny * nx
+    est_steps = per_interval * n_out
+    free, _ = torch.cuda.mem_get_info(dev)
+    timings = {}
+    best, best_ms = None, None
+    for k in CHECKPOINT_CHOICES:
+        if k % GRAPH_STEPS:
+            continue
+        need = (2 * k + 1 + -(-est_steps // k)) * state_bytes
+        if need > budget_frac * free and best is not None:
+            continue
+        U = Ud.clone().requires_grad_(True)
+        L = lv_t.clone().requires_grad_(True)
+        ms = []
+        with torch.enable_grad():
+            for rep in range(2):  # the first run captures the graphs
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                g, _ = gauge_run(model, U, L, out_dt, gauges, max_dt_cap=max_dt_cap,
+                                 checkpoint_every=k, store_states=store_states)
+                g.square().sum().backward()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms.append(e0.elapsed_time(e1))
+        timings[str(k)] = ms[-1]
+        if best_ms is None or ms[-1] < best_ms:
+            best, best_ms = k, ms[-1]
+    table[key] = {"k": int(best), "timing_ms": timings, "intervals_timed": n_t}
+    _store(dev, entry)
+    return int(best)
+
+
+def checkpoint_tuning(device, key_prefix: str = "") -> dict:
+    """The cached checkpoint-interval choices (and their timings) of a device."""
+    return {k: v for k, v in _load(device).get("checkpoint_every", {}).items() if k.startswith(key_prefix)}
+
+
 class sweep_rows:
     """Context manager: the single-grid kernels use ``rows`` inside (e.g.
     while a CUDA graph is captured), the previous value after."""
@@ -266,5 +339,6 @@ def apply(device="cuda", cells: Optional[int] = None, arithmetic: str = "exact")
 
 
 __all__ = ["tune", "tuned_rows", "tuned_ensemble_rows", "tuned_rows_for_shape", "sweep_rows", "apply",
+           "tuned_checkpoint_every", "checkpoint_tuning", "CHECKPOINT_CHOICES",
            "size_class",
            "SIZE_CLASSES", "ROW_CHOICES"]

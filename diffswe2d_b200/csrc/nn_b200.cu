@@ -8,8 +8,13 @@
 // deep; one elected thread issues the MMAs and commits them to an mbarrier
 // per stage; the epilogue reads the accumulator with tcgen05.ld (each warp
 // its 32 lanes) and applies bias and activation.  Every mbarrier wait is
-// bounded in time: past the limit the CTA records an error, waits (bounded)
-// for its issued MMAs, frees its tensor memory and returns.
+// bounded in time: a wait inside the K loop gives up after the launch's
+// limit (wait_ns), after which the CTA records error bit 1, stops issuing,
+// waits for its issued MMAs to drain (a fixed, separate bound of 2 s),
+// frees its tensor memory and returns.  If the drain bound also runs out,
+// the CTA still frees its tensor memory (every allocation must be freed
+// before the CTA exits) and records error bit 2: MMAs may then have been
+// running when it was freed, and the context should not be trusted.
 //
 // The rest are small memory-bound kernels (im2col / col2im for the 1D
 // convolutions, activation adjoint, transposes, column sums, MSE, Adam).
@@ -33,7 +38,10 @@ constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 // Two stages use 64 KB; the allocation is 96 KB so that the operand reads
 // of every descriptor stay inside it by a wide margin.
 constexpr int SMEM_BYTES = 96 * 1024;
-constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
+// Bound of the final wait for the CTA's own MMAs before its tensor memory is
+// freed (independent of the launch's wait limit, so that a short limit
+// never frees tensor memory under MMAs that are still running).
+constexpr unsigned long long DRAIN_LIMIT_NS = 2000000000ull;  // 2 s
 
 struct GemmArgs {
     const uint16_t* A;
@@ -46,6 +54,7 @@ struct GemmArgs {
     float* pre_f32;
     float* partial;  // split K: [z][M][N]
     uint32_t* err;
+    unsigned long long wait_ns;  // limit of each wait inside the K loop
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -90,13 +99,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase `parity` of an mbarrier.
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait for the phase `parity` of an mbarrier, giving up once `limit`
+// nanoseconds have passed (the time is checked before every probe, so a
+// limit of 0 gives up at once).
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit) {
     const unsigned long long t0 = global_ns();
-    while (!mbar_try(bar, parity)) {
-        if (global_ns() - t0 > WAIT_LIMIT_NS) return false;
+    while (global_ns() - t0 < limit) {
+        if (mbar_try(bar, parity)) return true;
     }
-    return true;
+    return false;
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
@@ -184,7 +195,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_kernel(const GemmArgs g) {
         uint8_t* sB = sA + A_BYTES;
         if (kb >= 2) {  // the MMAs that read this stage two blocks ago are done
             if (tid == 0) {
-                if (!mbar_wait(smem_u32(&s_bar[s]), phase[s])) s_ok = 0;
+                if (!mbar_wait(smem_u32(&s_bar[s]), phase[s], g.wait_ns)) s_ok = 0;
             }
             phase[s] ^= 1u;
             __syncthreads();
@@ -229,17 +240,19 @@ __global__ void __launch_bounds__(NT, 1) gemm_kernel(const GemmArgs g) {
     }
 
     // Wait for the last commit (it covers every MMA this thread issued).
+    __shared__ int s_drained;
+    if (tid == 0) s_drained = 1;
     if (issued > 0) {
         const int s = (issued - 1) & 1;
         if (tid == 0) {
-            if (!mbar_wait(smem_u32(&s_bar[s]), phase[s])) s_ok = 0;
+            if (!mbar_wait(smem_u32(&s_bar[s]), phase[s], DRAIN_LIMIT_NS)) s_drained = 0;
         }
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool ok = s_ok != 0;
+    const bool ok = s_ok != 0 && s_drained != 0;
     if (!ok) {
-        if (tid == 0 && g.err) atomicOr(g.err, 1u);
+        if (tid == 0 && g.err) atomicOr(g.err, (s_ok ? 0u : 1u) | (s_drained ? 0u : 2u));
     } else {
         const int r = m0 + warp * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -442,10 +455,11 @@ using namespace nn;
 
 extern "C" int nn_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M, int N,
                             int K, const float* bias, int act, float* out_f32, uint16_t* out_bf16,
-                            float* pre_f32, int ldc, int ksplit, float* workspace, uint32_t* err,
-                            void* stream) {
+                            float* pre_f32, int ldc, int ksplit, float* workspace,
+                            long long wait_ns, uint32_t* err, void* stream) {
     if (!A || !B || M < 1 || N < 1 || K < 16 || K % 16 || lda % 8 || ldb % 8 || lda < K || ldb < K)
         return SWE_EARG;
+    if (wait_ns < 0) return SWE_EARG;
     if (((uintptr_t)A | (uintptr_t)B) & 15u) return SWE_EARG;
     if (act != NN_ACT_NONE && act != NN_ACT_GELU) return SWE_EARG;
     if (!out_f32 && !out_bf16 && !pre_f32) return SWE_EARG;
@@ -479,6 +493,7 @@ extern "C" int nn_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int l
     g.pre_f32 = pre_f32;
     g.partial = zs > 1 ? workspace : nullptr;
     g.err = err;
+    g.wait_ns = (unsigned long long)wait_ns;
     cudaStream_t s = (cudaStream_t)stream;
     const dim3 grid((M + BM - 1) / BM, (N + BN_MAX - 1) / BN_MAX, zs);
     gemm_kernel<<<grid, NT, SMEM_BYTES, s>>>(g);

@@ -390,7 +390,7 @@ _WORKSPACES = {}
 
 def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
               gauges: Sequence[Tuple[int, int]], max_dt_cap=None, max_steps: int = 1_000_000,
-              graph_steps: int = GRAPH_STEPS, checkpoint_every: int = CHECKPOINT_EVERY,
+              graph_steps: int = GRAPH_STEPS, checkpoint_every: Optional[int] = CHECKPOINT_EVERY,
               store_states: Optional[bool] = None):
     """Advance ``U0`` through ``n_out`` output intervals of ``out_dt``
     seconds; interval i runs exactly like ``model(U, t_end=out_dt,
@@ -400,7 +400,15 @@ def gauge_run(model, U0: torch.Tensor, levels: torch.Tensor, out_dt: float,
     Returns ``(gauges, U_final)``: eta = h + bed at the gauge cells (row,
     column) after every interval, [B, n_out, len(gauges)], and the final
     state.  Differentiable with respect to U0, levels, the roughness field
-    and (when the DEM correction requires grad) the bed."""
+    and (when the DEM correction requires grad) the bed.
+
+    ``checkpoint_every=None`` takes the interval from the autotuner
+    (``autotune.tuned_checkpoint_every``: timed on this run's shape the first
+    time, then cached)."""
+    if checkpoint_every is None:
+        from .autotune import tuned_checkpoint_every
+        checkpoint_every = tuned_checkpoint_every(model, U0, levels, out_dt, gauges,
+                                                  max_dt_cap=max_dt_cap, store_states=store_states)
     model._check_state(U0)
     U0 = nat.require_cuda_f32("U0", U0)
     B, _, ny, nx = U0.shape

@@ -90,6 +90,7 @@ class InversionProblem:
     targets: Optional[torch.Tensor] = None  # [B, n_out, n_gauges]
     lo: float = BC_MINIMUM
     hi: float = BC_MAXIMUM
+    checkpoint_every: Optional[int] = None  # None: the autotuner's choice for this run
 
     @property
     def batch(self) -> int:
@@ -112,10 +113,16 @@ class InversionProblem:
         """Gauge eta [B, n_out, n_gauges] after each output chunk; the chunk's
         level is series[:, i] (held over the chunk, as the reference does).
         One gauge_run: a device-driven run with a checkpointed adjoint."""
+        if self.checkpoint_every is None:
+            from .autotune import tuned_checkpoint_every
+            self.checkpoint_every = tuned_checkpoint_every(self.model, self.U0, series, self.dt_out,
+                                                           self.gauges)
         if differentiable:
-            return gauge_run(self.model, self.U0, series, self.dt_out, self.gauges)[0]
+            return gauge_run(self.model, self.U0, series, self.dt_out, self.gauges,
+                             checkpoint_every=self.checkpoint_every)[0]
         with torch.no_grad():
-            return gauge_run(self.model, self.U0, series.detach(), self.dt_out, self.gauges)[0]
+            return gauge_run(self.model, self.U0, series.detach(), self.dt_out, self.gauges,
+                             checkpoint_every=self.checkpoint_every)[0]
 
     def simulate_chunked(self, series: torch.Tensor, differentiable: bool = True) -> torch.Tensor:
         """The same run as the reference's script writes it: one forward()

@@ -116,6 +116,8 @@ class WarmStartNet:
         self.v = torch.zeros_like(self.params)
         self.step_count = 0
         self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        #: limit of each tensor-core wait of the GEMM kernel (nn_gemm_bf16)
+        self.wait_ns = nat.NN_GEMM_WAIT_NS
         g = torch.Generator().manual_seed(seed)
         host = torch.zeros(self.nparams)
         for L, (w, rows, kp, b) in zip(self.layers, self.layout):
@@ -172,8 +174,8 @@ class WarmStartNet:
             ws = self._ws
         rc = nat.lib().nn_gemm_bf16(nat.ptr(A), lda, nat.ptr(B), ldb, M, N, K, nat.ptr(bias), act,
                                     nat.ptr(out_f32), nat.ptr(out_bf16), nat.ptr(pre),
-                                    N if ldc is None else ldc, ksplit, nat.ptr(ws), nat.ptr(self.err),
-                                    self._st())
+                                    N if ldc is None else ldc, ksplit, nat.ptr(ws), self.wait_ns,
+                                    nat.ptr(self.err), self._st())
         nat.check(rc, "nn gemm")
 
     @staticmethod
@@ -327,6 +329,9 @@ class WarmStartNet:
 
     def check_errors(self):
         code = int(self.err.item())
+        if code & 2:
+            raise RuntimeError(f"nn_gemm_bf16: tensor-core work had not finished when its tensor "
+                               f"memory was freed (code {code:#x}); the CUDA context is suspect")
         if code != 0:
             raise RuntimeError(f"a bounded wait in nn_gemm_bf16 ran past its time limit (code {code:#x})")
 

@@ -33,12 +33,20 @@ extern "C" {
  * pre-activation (A B^T + bias).  bias [N] fp32 or NULL.
  * ksplit > 1 splits K over that many CTAs (for small M, N and long K); the
  * partial sums go to `workspace` (ksplit * M * N floats) and a second kernel
- * adds them in a fixed order and applies the epilogue.  err (one word, may
- * be NULL) receives 1 if a tensor-core wait ran past its time limit.
+ * adds them in a fixed order and applies the epilogue.
+ * Every wait of a CTA for its tensor-core work inside the K loop gives up
+ * after wait_ns nanoseconds (>= 0; the time is checked before each probe,
+ * so 0 gives up at once; NN_GEMM_WAIT_NS is the normal limit); the CTA then
+ * stops, waits up to 2 s for the MMAs it issued, frees its tensor memory and
+ * returns without writing its tile.  err (one word, may be NULL) receives
+ * bit 1 when a wait gave up and bit 2 when the MMAs had still not completed
+ * when the tensor memory was freed (the context is then suspect).
  */
+#define NN_GEMM_WAIT_NS 1000000000LL
 int nn_gemm_bf16(const uint16_t* A, int lda, const uint16_t* B, int ldb, int M, int N, int K,
                  const float* bias, int act, float* out_f32, uint16_t* out_bf16, float* pre_f32,
-                 int ldc, int ksplit, float* workspace, uint32_t* err, void* stream);
+                 int ldc, int ksplit, float* workspace, long long wait_ns, uint32_t* err,
+                 void* stream);
 
 /*
  * Conv1d as a matrix: cols[(n*Lout + l), kk*Cin + ci] = scale * X[n, l*stride - pad + kk, ci]

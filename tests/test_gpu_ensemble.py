@@ -93,3 +93,36 @@ def test_gauge_ensemble_matches_gauge_run_per_member():
     capped = GaugeEnsemble(bed, n, U0, levels, out_dt, gauges, cfg, sc.dx, max_steps=5)
     with pytest.raises(RuntimeError, match="step cap"):
         capped.run()
+
+
+def test_nan_member_fails_alone():
+    """A member that starts with a NaN fails by itself (status non-finite
+    state); every other member runs to its end, bit for bit as alone."""
+    members = _members()[:4]
+    bad = 2
+    members[bad].U0 = members[bad].U0.copy()
+    members[bad].U0[0, 0, 5, 7] = float("nan")
+    res = Ensemble(members, device=DEV, rows=8).run(strict=False)
+    assert res.failed == [bad]
+    assert res.status[bad] & 1  # SWE_S_NONFINITE_STATE
+    for m, sc in enumerate(members):
+        if m == bad:
+            continue
+        U, t = _alone(sc)
+        assert res.steps[m] == sc.steps and res.status[m] == 0
+        assert torch.equal(res.states[m], U), f"scenario {m}"
+    with pytest.raises(FloatingPointError, match="scenario 2"):
+        Ensemble(members, device=DEV, rows=8).run()
+
+
+def test_idle_limit_surfaces_as_error_and_kernel_returns():
+    """The persistent kernel's idle limit at one microsecond: blocks that find
+    no work see no phase completed within it (a phase takes longer), set the
+    launch's error bit and leave; the launch ends and the error surfaces as
+    a Python exception.  The same ensemble with the default limit runs."""
+    sc = scenarios.ensemble_member(96, 96, seed=7)
+    sc.steps = 40
+    with pytest.raises(RuntimeError, match="idle limit"):
+        Ensemble([sc], device=DEV, rows=8, stall_ns=1000).run()
+    res = Ensemble([sc], device=DEV, rows=8).run()
+    assert res.steps == [40]

@@ -134,3 +134,35 @@ def test_bed_gradient_matches_chunked_autograd(store):
     a, b = out
     assert np.abs(b).max() > 0
     assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+
+
+def test_tuned_checkpoint_interval(tmp_path, monkeypatch):
+    """checkpoint_every=None: the autotuner times the run for every k of
+    CHECKPOINT_CHOICES, caches the fastest and the run uses it; gradients do
+    not depend on k (bit for bit), so the choice is purely a speed one."""
+    from diffswe2d_b200 import autotune
+    from diffswe2d_b200.gauge_run import _WORKSPACES
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    monkeypatch.setattr(autotune, "_tuned", {})
+    m, U0 = _model(2)
+    levels = _levels(2, 40)
+    U = U0.clone().requires_grad_(True)
+    L = levels.clone().requires_grad_(True)
+    g, _ = gauge_run(m, U, L, 0.25, GAUGES, checkpoint_every=None)
+    g.square().sum().backward()
+    ws = list(_WORKSPACES.values())[0]
+    assert ws.k in autotune.CHECKPOINT_CHOICES
+    tuned = autotune.checkpoint_tuning(DEV)
+    assert len(tuned) == 1 and list(tuned.values())[0]["k"] == ws.k
+    monkeypatch.setattr(autotune, "_tuned", {})  # the cache is read back from disk
+    assert autotune.tuned_checkpoint_every(m, U0, levels, 0.25, GAUGES) == ws.k
+    grads = []
+    for k in (32, 256):
+        U2 = U0.clone().requires_grad_(True)
+        L2 = levels.clone().requires_grad_(True)
+        g2, _ = gauge_run(m, U2, L2, 0.25, GAUGES, checkpoint_every=k)
+        g2.square().sum().backward()
+        assert torch.equal(g2, g)
+        grads.append((U2.grad, L2.grad))
+    assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
+    assert torch.equal(grads[0][0], U.grad) and torch.equal(grads[0][1], L.grad)
