@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-reference-context", action="store_true",
                     help="skip timing the reference's own PyTorch step (baseline/_ref)")
     ap.add_argument("--reference-context", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--rows", type=int, default=0,
+                    help="sweep tile height to use instead of the autotuner's (0: autotune)")
     ap.add_argument("--workload", choices=["runup4096", "ensemble", "inversion", "warmstart"],
                     default="runup4096",
                     help="runup4096: the headline single-grid step; ensemble: 64 scenarios of "
@@ -279,8 +281,11 @@ def time_single_grid(sc, args, dev, arithmetic, clocks=None):
     ny, nx = sc.bed.shape
     cells = ny * nx
     cfg = SWEConfig(**sc.config)
-    tuning = autotune.tune(dev, arithmetic=arithmetic)
-    rows = autotune.tuned_rows(cells, dev, arithmetic)
+    if args.rows > 0:
+        tuning, rows = {}, args.rows
+    else:
+        tuning = autotune.tune(dev, arithmetic=arithmetic)
+        rows = autotune.tuned_rows(cells, dev, arithmetic)
     lib = nat.lib()
     nat.check(lib.swe_tune_sweep_rows(rows), "tuned rows")
     p = nat.params(cfg, sc.dx, sc.dy, arithmetic)
@@ -393,8 +398,12 @@ def reference_context(args, timeout_s=420):
     cmd = [sys.executable, str(Path(__file__).resolve()), "--reference-context",
            "--ny", str(args.ny), "--nx", str(args.nx)]
     note = None
+    env = dict(os.environ)
+    for var, path in (("CC", "/usr/bin/gcc"), ("CXX", "/usr/bin/g++")):  # compilers with OpenMP
+        if os.path.exists(path):
+            env[var] = path
     try:
-        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
         stdout, stderr = out.stdout, out.stderr
     except subprocess.TimeoutExpired as e:
         stdout = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
@@ -486,23 +495,32 @@ def run_reference_context(args):
     res["cuda_eager"] = {"value": timed(eager, 10), "unit": "Mcell-updates/s",
                          "sample": f"10 steps of the {ny}x{nx} grid"}
     print(json.dumps(res), flush=True)
-    # the reference's own usage: torch.compile(model) around forward()
-    cm = torch.compile(m)
-    dt0 = float(m.stable_dt(U0, boundary_level=m._interpolate_dynamic_boundary(t0, U0)))
-    start = time.perf_counter()
+    # the reference's own usage: torch.compile(model) around forward(), with
+    # the boundary level given per call as its inversion script does (the
+    # series lookup of _interpolate_dynamic_boundary does not trace)
+    level0 = level_at(sc, t0)
+    dt0 = float(m.stable_dt(U0, boundary_level=level0))
     counted = []
+    try:
+        cm = torch.compile(m)
+        start = time.perf_counter()
 
-    def compiled(count):
-        counted.clear()
-        with torch.no_grad():
-            cm(U0, t_end=count * dt0, start_time=t0, callback=lambda i, t, U: counted.append(i))
-        return len(counted)
+        def compiled(count):
+            counted.clear()
+            with torch.no_grad():
+                cm(U0, t_end=count * dt0, start_time=t0, boundary_level=level0,
+                   callback=lambda i, t, U: counted.append(i))
+            return len(counted)
 
-    compiled(3)
-    res["cuda_compile_seconds"] = time.perf_counter() - start
-    res["cuda_compile"] = {"value": timed(compiled, 10), "unit": "Mcell-updates/s",
-                           "sample": f"forward() of about 10 steps of the {ny}x{nx} grid, "
-                                     "torch.compile(model) as the reference's examples do"}
+        compiled(3)
+        res["cuda_compile_seconds"] = time.perf_counter() - start
+        res["cuda_compile"] = {"value": timed(compiled, 10), "unit": "Mcell-updates/s",
+                               "sample": f"forward() of about 10 steps of the {ny}x{nx} grid, "
+                                         "torch.compile(model) as the reference's examples do"}
+    except Exception as e:  # report why, keep the other numbers
+        lines = [l for l in str(e).splitlines() if l.strip()]
+        res["cuda_compile"] = {"unavailable": f"torch.compile of the reference failed: "
+                                              f"{type(e).__name__}: {(lines or ['?'])[0][:300]}"}
     print(json.dumps(res), flush=True)
 
 
