@@ -113,16 +113,18 @@ class InversionProblem:
         """Gauge eta [B, n_out, n_gauges] after each output chunk; the chunk's
         level is series[:, i] (held over the chunk, as the reference does).
         One gauge_run: a device-driven run with a checkpointed adjoint."""
-        if self.checkpoint_every is None:
-            from .autotune import tuned_checkpoint_every
-            self.checkpoint_every = tuned_checkpoint_every(self.model, self.U0, series, self.dt_out,
-                                                           self.gauges)
         if differentiable:
+            if self.checkpoint_every is None:
+                from .autotune import tuned_checkpoint_every
+                self.checkpoint_every = tuned_checkpoint_every(self.model, self.U0, series,
+                                                               self.dt_out, self.gauges)
             return gauge_run(self.model, self.U0, series, self.dt_out, self.gauges,
                              checkpoint_every=self.checkpoint_every)[0]
+        # a forward-only run keeps no segments: k only sets the checkpoint copies
+        from .gauge_run import CHECKPOINT_EVERY
         with torch.no_grad():
             return gauge_run(self.model, self.U0, series.detach(), self.dt_out, self.gauges,
-                             checkpoint_every=self.checkpoint_every)[0]
+                             checkpoint_every=self.checkpoint_every or CHECKPOINT_EVERY)[0]
 
     def simulate_chunked(self, series: torch.Tensor, differentiable: bool = True) -> torch.Tensor:
         """The same run as the reference's script writes it: one forward()
@@ -214,6 +216,7 @@ class RunupFamily:
     n_gauges: int = 6
     bathy_perturb: float = 0.01
     device: str = "cuda"
+    arithmetic: str = "exact"  # step kernels of the runs and inversions ("exact" or "fast")
 
     def __post_init__(self):
         from . import scenarios
@@ -255,7 +258,8 @@ class RunupFamily:
         from .solver import SWE2D
         bed = torch.tensor(beds[:, None], device=self.device)
         n = torch.full_like(bed, 0.01)
-        model = SWE2D(bed, n, self.dx, self.dx, config=self.config, train_dem=False)
+        model = SWE2D(bed, n, self.dx, self.dx, config=self.config, train_dem=False,
+                      arithmetic=self.arithmetic)
         h0 = torch.clamp(-bed, min=0.0)
         U0 = torch.cat([h0, torch.zeros_like(h0), torch.zeros_like(h0)], dim=1).contiguous()
         problem = InversionProblem(model, U0, self.gauges, self.dt_out, self.n_out, self.basis)
@@ -278,7 +282,7 @@ class RunupFamily:
             v = torch.as_tensor(values[s:s + 1024], device=self.device)
             levels = (v @ self.basis.t()).contiguous()
             ens = GaugeEnsemble(bed, n, U0, levels, self.dt_out, self.gauges, self.config, self.dx,
-                                rows=rows)
+                                rows=rows, arithmetic=self.arithmetic)
             res = ens.run()
             out.append(res.gauges)
             self.last_ensemble = res

@@ -32,4 +32,27 @@ def reduce_over_ranks(values: Sequence[float], op: str, device=None) -> List[flo
     return [float(v) for v in t.cpu()]
 
 
-__all__ = ["shard_indices", "reduce_over_ranks"]
+def gather_rows(count: int, mine: Sequence[int], tensors: Sequence, world: int) -> List:
+    """Each rank holds rows `mine` (indices into `count` units) of some
+    tensors; returns on every rank the full tensors [count, ...] in unit
+    order (one all_gather of the host copies, once, at the end of a run)."""
+    import torch.distributed as dist
+    local = [None if t is None else t.detach().cpu() for t in tensors]
+    parts = [None] * world
+    dist.all_gather_object(parts, (list(mine), local))
+    device = next((t.device for t in tensors if t is not None), torch.device("cpu"))
+    out = []
+    for j in range(len(tensors)):
+        rows = {}
+        for idx, ts in parts:
+            if ts[j] is None:
+                continue
+            for r, i in enumerate(idx):
+                rows[i] = ts[j][r]
+        if len(rows) != count:
+            raise RuntimeError(f"gathered {len(rows)} of {count} units")
+        out.append(torch.stack([rows[i] for i in range(count)]).to(device))
+    return out
+
+
+__all__ = ["shard_indices", "reduce_over_ranks", "gather_rows"]

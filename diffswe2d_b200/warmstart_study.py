@@ -33,20 +33,46 @@ class Dataset:
     cell_updates: int
 
 
-def generate(fam: RunupFamily, count: int, seed: int, rows: Optional[int] = None) -> Dataset:
-    rng = np.random.default_rng(seed)
+def run_inputs(fam: RunupFamily, index: int, seed: int):
+    """Bed [ny, nx] and control values [n_controls] of run `index`: drawn from
+    a generator seeded by (seed, index), so a run does not depend on which
+    rank makes it or in which batch."""
+    rng = np.random.default_rng([seed, index])
+    return fam.beds(1, rng)[0], fam.controls(1, rng)[0]
+
+
+def generate(fam: RunupFamily, count: int, seed: int, rows: Optional[int] = None,
+             world: int = 1, rank: int = 0, simulate=None) -> Dataset:
+    """`count` training runs; with world > 1 each rank runs its round-robin
+    share (no communication during the runs) and the dataset is gathered
+    once at the end, in run order, on every rank -- the same dataset as one
+    rank makes.  `simulate(beds, values) -> gauges [m, n_out, G]` defaults
+    to the family's persistent ensemble launch."""
+    from .sharding import gather_rows, shard_indices
+    mine = shard_indices(count, world, rank)
+    sim = simulate or (lambda b, v: fam.ensemble_gauges(b, v, rows=rows))
     xs, ys, cells = [], [], 0
     t0 = time.perf_counter()
-    for s in range(0, count, 1024):
-        m = min(1024, count - s)
-        beds = fam.beds(m, rng)
-        values = fam.controls(m, rng)
-        g = fam.ensemble_gauges(beds, values, rows=rows)   # [m, n_out, G]
+    for s in range(0, len(mine), 1024):
+        part = [run_inputs(fam, k, seed) for k in mine[s:s + 1024]]
+        beds = np.stack([p[0] for p in part])
+        values = np.stack([p[1] for p in part])
+        g = sim(beds, values)   # [m, n_out, G]
         xs.append(g.transpose(1, 2).contiguous())
         ys.append(torch.as_tensor(values, device=g.device))
-        cells += fam.last_ensemble.cell_updates
-    torch.cuda.synchronize()
-    return Dataset(torch.cat(xs), torch.cat(ys), time.perf_counter() - t0, cells)
+        if simulate is None:
+            cells += fam.last_ensemble.cell_updates
+    x = torch.cat(xs) if xs else None
+    y = torch.cat(ys) if ys else None
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    if world > 1:
+        x, y = gather_rows(count, mine, [x, y], world)
+        from .sharding import reduce_over_ranks
+        seconds = reduce_over_ranks([seconds], "max")[0]
+        cells = int(reduce_over_ranks([cells], "sum")[0])
+    return Dataset(x, y, seconds, cells)
 
 
 @dataclass
@@ -128,6 +154,107 @@ def compare(fam: RunupFamily, net: WarmStartNet, cases: int, seed: int, lr: floa
     }
 
 
+def compare_at_scale(fam: RunupFamily, net: WarmStartNet, cases: int, seed: int, lr: float = 0.002,
+                     tol: float = 1e-4, warm_max_iters: int = 20, cold_cases: int = 8,
+                     cold_max_iters: int = 40, world: int = 1, rank: int = 0) -> Dict:
+    """The comparison for grids where a batched adjoint iteration over every
+    held-out case costs minutes: the warm start is evaluated on all `cases`
+    (one batched forward run of the predicted controls; only the cases not
+    yet within `tol` are inverted further, as a batch, for up to
+    `warm_max_iters` iterations), the cold start on the first `cold_cases`
+    of them for up to `cold_max_iters` iterations (its cost per case is the
+    same for every case: each iteration is one forward + adjoint run).
+    Held-out case c is drawn from a generator seeded by (seed, c); with
+    world > 1 each rank takes its round-robin share of the cases and the
+    per-case results are gathered once at the end.  Times are this rank's
+    wall times, shared out per case of a batch."""
+    from .sharding import shard_indices
+    mine = shard_indices(cases, world, rank)
+    recs = {}
+    t_inf = 0.0
+    if mine:
+        inputs = [run_inputs(fam, c, seed) for c in mine]
+        beds = np.stack([p[0] for p in inputs])
+        truth = np.stack([p[1] for p in inputs])
+        problem = fam.problem(beds, truth)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pred = net.predict_controls(problem.targets.transpose(1, 2).contiguous())
+        eps = 1e-4
+        warm_vals = pred.clamp(problem.lo + eps, problem.hi - eps)
+        torch.cuda.synchronize()
+        t_inf = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        with torch.no_grad():
+            sim = problem.simulate(problem.series(raw_from_controls(warm_vals)), differentiable=False)
+        rmse0 = ((sim - problem.targets) ** 2).mean(dim=(1, 2)).sqrt().cpu().numpy()
+        torch.cuda.synchronize()
+        per_case_eval = (time.perf_counter() - t0) / len(mine)
+        err2 = ((pred - torch.as_tensor(truth, device=pred.device)) ** 2).sum(dim=1).cpu().numpy()
+        for j, c in enumerate(mine):
+            ok = bool(rmse0[j] <= tol)
+            recs[c] = {"rmse0": float(rmse0[j]), "warm_it": 0 if ok else None,
+                       "warm_s": t_inf / len(mine) + per_case_eval if ok else None,
+                       "eval_s": per_case_eval, "err2": float(err2[j])}
+        left = [j for j, c in enumerate(mine) if rmse0[j] > tol]
+        if left and warm_max_iters > 0:
+            sub = fam.problem(beds[left], truth[left])
+            res = invert(sub, raw_from_controls(warm_vals[left]), lr=lr, max_iters=warm_max_iters,
+                         rmse_tol=tol)
+            for q, j in enumerate(left):
+                r = recs[mine[j]]
+                r["warm_iter_s"] = res.seconds_per_iteration / len(left)
+                if res.iterations_to_tol[q] is not None:
+                    r["warm_it"] = res.iterations_to_tol[q]
+                    r["warm_s"] = t_inf / len(mine) + per_case_eval + res.seconds_to_tol[q] / len(left)
+        cold_local = [j for j, c in enumerate(mine) if c < cold_cases]
+        if cold_local:
+            cold = fam.problem(beds[cold_local], truth[cold_local])
+            raw0 = raw_from_controls(torch.zeros((len(cold_local), fam.n_controls),
+                                                 device=problem.U0.device))
+            rc = invert(cold, raw0, lr=lr, max_iters=cold_max_iters, rmse_tol=tol)
+            for q, j in enumerate(cold_local):
+                recs[mine[j]].update(cold_it=rc.iterations_to_tol[q],
+                                     cold_iter_s=rc.seconds_per_iteration / len(cold_local),
+                                     cold_rmse0=rc.rmse_history[0][q], cold_rmse=rc.rmse_history[-1][q])
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, (recs, t_inf))
+        recs = {k: v for part, _ in parts for k, v in part.items()}
+        t_inf = max(t for _, t in parts)
+    order = list(range(cases))
+    warm_iters = [recs[c]["warm_it"] for c in order]
+    reached = [i for i in warm_iters if i is not None]
+    cold = [recs[c] for c in order if "cold_it" in recs[c]]
+    iter_s = [r["warm_iter_s"] for r in recs.values() if "warm_iter_s" in r]
+    return {
+        "cases": cases, "tol_m": tol, "lr": lr, "inference_s": t_inf,
+        "pred_control_rmse_m": float(np.sqrt(sum(recs[c]["err2"] for c in order)
+                                             / (cases * fam.n_controls))),
+        "warm": {
+            "reached": len(reached),
+            "reached_at_iteration_0": int(sum(1 for i in warm_iters if i == 0)),
+            "median_iterations": float(np.median(reached)) if reached else None,
+            "iterations": warm_iters,
+            "seconds_to_tol": [recs[c]["warm_s"] for c in order],
+            "initial_rmse": [recs[c]["rmse0"] for c in order],
+            "forward_eval_s_per_case": float(np.mean([recs[c]["eval_s"] for c in order])),
+            "seconds_per_iteration_per_case": float(np.mean(iter_s)) if iter_s else None,
+            "max_iters": warm_max_iters,
+        },
+        "cold": {
+            "cases": len(cold), "max_iters": cold_max_iters,
+            "reached": sum(1 for r in cold if r["cold_it"] is not None),
+            "iterations": [r["cold_it"] for r in cold],
+            "seconds_per_iteration_per_case": float(np.mean([r["cold_iter_s"] for r in cold]))
+            if cold else None,
+            "initial_rmse": [r["cold_rmse0"] for r in cold],
+            "final_rmse": [r["cold_rmse"] for r in cold],
+        },
+    }
+
+
 def _summary(res, extra_s: float) -> Dict:
     its = res.iterations_to_tol
     reached = [i for i in its if i is not None]
@@ -143,4 +270,4 @@ def _summary(res, extra_s: float) -> Dict:
     }
 
 
-__all__ = ["Dataset", "generate", "train", "compare", "TrainLog"]
+__all__ = ["Dataset", "generate", "train", "compare", "compare_at_scale", "TrainLog"]
