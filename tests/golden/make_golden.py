@@ -5,7 +5,7 @@ environment variable DIFFSWE2D_REFERENCE; the fixtures it writes are what the
 tests read, so the reference itself never has to be present where the tests
 run:
 
-    python tests/golden/make_golden.py --ref <reference checkout> [--only ops,c1,c2,forcing,adj]
+    python tests/golden/make_golden.py --ref <reference checkout> [--only ops,c1,c2,forcing,cea,adj]
 
 The reference is imported as the package ``diffswe2d`` from its ``src/``
 directory.  Its ``io_netcdf`` module imports ``xarray`` at load time, which
@@ -21,6 +21,8 @@ Fixtures (numpy .npz, float32 unless noted):
   adj_step.npz, adj_run.npz   reference autograd gradients (make_golden_adjoint.py)
   spline.npz      clamped B-spline basis and bounded controls of the
                   reference's inversion script
+  cea_topo.npz    the CEA 2008 DEM (an ESRI ASCII raster of the reference's
+                  examples) as the reference's io_ascii reader grids it
   forcing.npz     rainfall and infiltration sources: spatial_operator with
                   scalar / field / per-batch rates, steps with infiltration,
                   and steps of a model forced by RainfallForcing
@@ -346,6 +348,22 @@ def make_forcing(ref, out):
     print("forcing.npz", len(d), "arrays")
 
 
+def make_cea(ref_root, out):
+    """The CEA 2008 rainfall-runoff DEM (Examples/forward/Cea2008/
+    Cea2008_C1_new/topo.asc, ESRI ASCII) read and regridded by the
+    reference's own reader onto the example's model grid (example_run.py:
+    ModelGrid.from_bounds(0.02, 2.02, -0.005, 2.535, 0.01), float64)."""
+    import diffswe2d.io_ascii as io_ascii
+    from diffswe2d.io_netcdf import ModelGrid
+    path = pathlib.Path(ref_root) / "Examples/forward/Cea2008/Cea2008_C1_new/topo.asc"
+    grid = ModelGrid.from_bounds(xmin=0.02, xmax=2.02, ymin=-0.005, ymax=2.535, resolution=0.01,
+                                 dtype=torch.float64, device="cpu")
+    bed, spec = io_ascii.ascii_to_tensor(path, grid, dtype=torch.float64)
+    np.savez_compressed(out / "cea_topo.npz", bed=bed.numpy(), dx=np.float64(spec.resolution),
+                        bounds=np.array([spec.xmin, spec.xmax, spec.ymin, spec.ymax]))
+    print("cea_topo.npz", tuple(bed.shape))
+
+
 def main():
     import os
     ap = argparse.ArgumentParser()
@@ -366,6 +384,8 @@ def main():
         make_c2(ref, HERE)
     if "forcing" in groups:
         make_forcing(ref, HERE)
+    if "cea" in groups:
+        make_cea(args.ref, HERE)
     if "adj" in groups:
         from make_golden_adjoint import make_adjoint  # noqa: E402
         make_adjoint(ref, HERE)

@@ -204,3 +204,12 @@ def test_steps_with_rainfall_forcing(golden):
         t += dt
     assert np.array_equal(U, d["stcr_rainfall"])
     assert np.array_equal(np.array(dts), d["stcr_rainfall_dts"])
+
+
+def test_cea_dem_fixture_from_the_reference_reader(golden):
+    """The CEA DEM as the reference's io_ascii reader grids it: the example's
+    254 x 200 grid at 0.01 m, finite, the raster's elevation range."""
+    d = golden("cea_topo")
+    bed = d["bed"]
+    assert bed.shape == (254, 200) and float(d["dx"]) == 0.01
+    assert np.isfinite(bed).all() and -0.51 < bed.min() and bed.max() < 0.11
