@@ -88,6 +88,8 @@ def parse():
                     help="inversion: runup cases inverted together")
     ap.add_argument("--inv-grid", default="244x393x0.014", help="inversion: ny x nx x dx")
     ap.add_argument("--inv-duration", type=float, default=22.5, help="inversion: seconds simulated")
+    ap.add_argument("--inv-arithmetic", choices=["exact", "fast"], default="fast",
+                    help="inversion: step kernels of the forward run and its recompute")
     ap.add_argument("--ws-train", type=int, default=20000, help="warmstart: training runs")
     ap.add_argument("--ws-cases", type=int, default=100, help="warmstart: held-out cases")
     ap.add_argument("--ws-epochs", type=int, default=30)
@@ -659,7 +661,8 @@ def run_inversion(args, world, rank, local):
     gy, gx, gdx = args.inv_grid.split("x")
     gy, gx, gdx = int(gy), int(gx), float(gdx)
     problem, raw_true = make_runup_problem(cases=args.inv_cases, seed=0, ny=gy, nx=gx, dx=gdx,
-                                           duration=args.inv_duration, dt_out=0.02, device=dev)
+                                           duration=args.inv_duration, dt_out=0.02, device=dev,
+                                           arithmetic=args.inv_arithmetic)
     raw = torch.zeros_like(raw_true).requires_grad_(True)
     opt = torch.optim.Adam([raw], lr=0.002)
     clk = Clocks(local)
@@ -695,6 +698,8 @@ def run_inversion(args, world, rank, local):
                    "controls": 16, "gauges": 6, "dt_out": 0.02, "duration_s": args.inv_duration,
                    "lr": 0.002,
                    "solver_steps_per_run": steps, "checkpoint_every": ws.k,
+                   "checkpoint_every_source": "autotuner (timed k in 32/64/128/256)",
+                   "arithmetic": args.inv_arithmetic,
                    "backward_states": "kept from the forward pass" if ws.stored
                    else "recomputed from checkpoints",
                    "l2": "per-iteration working set (states, checkpoints, face buffers) > L2"},

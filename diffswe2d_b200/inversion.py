@@ -293,12 +293,12 @@ class RunupFamily:
 def make_runup_problem(cases: int = 4, seed: int = 0, ny: int = 122, nx: int = 196,
                        dx: float = 0.028, duration: float = 22.5, dt_out: float = 0.1,
                        n_controls: int = 16, n_gauges: int = 6, device="cuda",
-                       bathy_perturb: float = 0.01):
+                       bathy_perturb: float = 0.01, arithmetic: str = "exact"):
     """Config 3 at a chosen resolution (a RunupFamily): `cases` perturbed beds
     and seeded true controls.  Returns (problem, true raw controls
     [cases, n_controls])."""
     fam = RunupFamily(ny, nx, dx, seed, duration, dt_out, n_controls, n_gauges, bathy_perturb,
-                      str(device))
+                      str(device), arithmetic)
     rng = np.random.default_rng(seed)
     beds = fam.beds(cases, rng)
     truth = fam.controls(cases, rng)

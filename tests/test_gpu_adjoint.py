@@ -79,10 +79,11 @@ def test_one_step_vjp_matches_reference_autograd(golden, case):
         assert _rel(gn, d[f"{case}_gn"]) <= TOL
 
 
-def _run_model(d, requires=True):
+def _run_model(d, requires=True, arithmetic="exact"):
     cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
                     boundary_bottom="wall")
-    m = SWE2D(_t(d["bed"]), _t(d["n"]), float(d["dx"]), float(d["dx"]), config=cfg, train_dem=False)
+    m = SWE2D(_t(d["bed"]), _t(d["n"]), float(d["dx"]), float(d["dx"]), config=cfg, train_dem=False,
+              arithmetic=arithmetic)
     m.roughness_length.requires_grad_(requires)
     return m
 
@@ -117,6 +118,28 @@ def test_thirty_step_gradients_match_reference_autograd(golden, fixture):
         "n": _rel(m.roughness_length.grad.cpu().numpy(), d["f64_gn"]),
     }
     print("vs reference autograd FP32", errs, "vs FP64", errs64)
+    for k, e in errs.items():
+        assert e <= TOL, k
+
+
+@pytest.mark.parametrize("fixture", ["adj_run", "adj_run_wet"])
+def test_thirty_step_gradients_with_fast_forward(golden, fixture):
+    """The tolerance-mode forward kernels (inversions run on them): the
+    adjoint, evaluated at their states, still matches the reference's
+    autograd to the 1e-4 bar."""
+    d = golden(fixture)
+    m = _run_model(d, arithmetic="fast")
+    U0 = _t(d["U0"]).requires_grad_(True)
+    lv = _t(d["levels"]).requires_grad_(True)
+    loss = _run_loss(m, U0, lv, d["gauges"], _t(d["bed"]))
+    loss.backward()
+    assert float(loss.detach()) == pytest.approx(float(d["f32_loss"]), rel=1e-5)
+    errs = {
+        "U0": _rel(U0.grad.cpu().numpy(), d["f32_gU0"]),
+        "levels": _rel(lv.grad.cpu().numpy(), d["f32_glevels"]),
+        "n": _rel(m.roughness_length.grad.cpu().numpy(), d["f32_gn"]),
+    }
+    print("fast forward: vs reference autograd FP32", errs)
     for k, e in errs.items():
         assert e <= TOL, k
 
