@@ -27,37 +27,31 @@ from .gauge_run import gauge_run
 
 # ------------------------------------------------------------------ spline
 def clamped_bspline_basis(sample_times: torch.Tensor, number_of_controls: int, degree: int = 3):
-    """Basis matrix [T, n], knot vector and Greville abscissae of a clamped
-    B-spline with uniform interior knots, by the Cox-de Boor recursion
-    (bc_inversion_train.py:189-231).  The last sample is assigned to the last
-    basis function so every row sums to one."""
-    if degree < 1 or number_of_controls < degree + 1:
-        raise ValueError("Require degree >= 1 and number_of_controls >= degree + 1.")
+    """Basis matrix [T, n], knot vector and Greville abscissae of the clamped
+    B-spline the reference's inversion script uses (bc_inversion_train.py:
+    189-231): ``degree + 1`` repeated knots at the first and last sample
+    time, ``n - degree - 1`` uniform interior knots.  The basis is SciPy's
+    B-spline design matrix (de Boor's algorithm) on the sample times, the
+    last sample belonging to the last interval, so every row sums to one;
+    the Greville abscissa of control i is the mean of knots i+1 .. i+degree."""
+    from scipy.interpolate import BSpline
+    if degree < 1:
+        raise ValueError(f"degree must be at least 1, got {degree}")
+    if number_of_controls < degree + 1:
+        raise ValueError(f"a degree-{degree} spline needs at least {degree + 1} controls, "
+                         f"got {number_of_controls}")
     if sample_times.ndim != 1 or sample_times.numel() < 2:
-        raise ValueError("sample_times must be a one-dimensional tensor with at least two values.")
-    t = sample_times.to(torch.float64)
-    t0, t1 = t[0], t[-1]
-    n_int = number_of_controls - degree - 1
-    interior = (torch.linspace(float(t0), float(t1), n_int + 2, dtype=torch.float64)[1:-1]
-                if n_int > 0 else t.new_empty(0))
-    knots = torch.cat((t0.repeat(degree + 1), interior, t1.repeat(degree + 1)))
-    x = t[:, None]
-    basis = ((x >= knots[:-1]) & (x < knots[1:])).to(torch.float64)
-    eps = torch.finfo(torch.float64).eps
-    for order in range(1, degree + 1):
-        cols = knots.numel() - order - 1
-        ld = knots[order:order + cols] - knots[:cols]
-        rd = knots[order + 1:order + 1 + cols] - knots[1:1 + cols]
-        left = torch.where(ld > 0, (x - knots[:cols]) / ld.clamp_min(eps), 0.0)
-        right = torch.where(rd > 0, (knots[order + 1:order + 1 + cols] - x) / rd.clamp_min(eps), 0.0)
-        basis = left * basis[:, :cols] + right * basis[:, 1:cols + 1]
-    basis[-1].zero_()
-    basis[-1, -1] = 1.0
-    if not torch.allclose(basis.sum(1), torch.ones(basis.shape[0], dtype=torch.float64),
-                          atol=1e-10, rtol=1e-10):
-        raise RuntimeError("B-spline basis does not form a partition of unity.")
-    greville = torch.stack([knots[i + 1:i + degree + 1].mean() for i in range(number_of_controls)])
-    return basis, knots, greville
+        raise ValueError("sample_times must be 1-D with at least two times")
+    t = sample_times.detach().to(torch.float64).cpu().numpy()
+    interior = np.linspace(t[0], t[-1], number_of_controls - degree + 1)[1:-1]
+    knots = np.concatenate([np.full(degree + 1, t[0]), interior, np.full(degree + 1, t[-1])])
+    basis = BSpline.design_matrix(t, knots, degree, extrapolate=False).toarray()
+    if not np.allclose(basis.sum(axis=1), 1.0, rtol=0, atol=1e-10):
+        raise RuntimeError("the B-spline basis rows do not sum to one")
+    greville = np.array([knots[i + 1:i + degree + 1].mean() for i in range(number_of_controls)])
+    dev = sample_times.device
+    return (torch.from_numpy(basis).to(dev), torch.from_numpy(knots).to(dev),
+            torch.from_numpy(greville).to(dev))
 
 
 BC_MINIMUM, BC_MAXIMUM = -0.02, 0.05
