@@ -84,6 +84,8 @@ def parse():
                          "uneven sizes in one persistent launch vs 64 sequential runs")
     ap.add_argument("--ensemble-steps", type=int, default=2000)
     ap.add_argument("--ensemble-count", type=int, default=64)
+    ap.add_argument("--ens-arithmetic", choices=["exact", "fast"], default="fast",
+                    help="ensemble: step kernels of the scenarios")
     ap.add_argument("--inv-cases", type=int, default=4,
                     help="inversion: runup cases inverted together")
     ap.add_argument("--inv-grid", default="244x393x0.014", help="inversion: ny x nx x dx")
@@ -588,8 +590,9 @@ def run_ensemble(args, world, rank, local):
         sc = scenarios.ensemble_member(ny, nx, seed=k)
         sc.steps = args.ensemble_steps
         members.append(sc)
-    tuning = tune(dev)
-    ens = Ensemble(members, device=dev)
+    arith = args.ens_arithmetic
+    tuning = tune(dev, arithmetic=arith)
+    ens = Ensemble(members, device=dev, arithmetic=arith)
     ens.run()  # warm-up (also captures the graph)
     if world > 1:
         import torch.distributed as dist
@@ -604,9 +607,9 @@ def run_ensemble(args, world, rank, local):
     from diffswe2d_b200.autotune import tuned_rows
     for sc in members:
         ny, nx = sc.bed.shape
-        nat.check(lib.swe_tune_sweep_rows(tuned_rows(ny * nx, dev)), "tuned rows")
+        nat.check(lib.swe_tune_sweep_rows(tuned_rows(ny * nx, dev, arith)), "tuned rows")
         cfg = SWEConfig(**sc.config)
-        p = nat.params(cfg, sc.dx, sc.dy)
+        p = nat.params(cfg, sc.dx, sc.dy, arith)
         bed = torch.from_numpy(sc.bed).to(dev)
         n = torch.from_numpy(sc.roughness).to(dev)
         U = [torch.from_numpy(sc.U0).to(dev), torch.empty((1, 3, ny, nx), device=dev)]
@@ -633,7 +636,9 @@ def run_ensemble(args, world, rank, local):
         "config": {"workload": f"ensemble_{args.ensemble_count}_sides_128_1024",
                    "scenarios": len(sizes), "steps_each": args.ensemble_steps,
                    "cells_total": int(sum(a * b for a, b in sizes)),
-                   "ensemble_tile_rows": tuning.get("ensemble_rows"),
+                   "ensemble_tile_rows": tuning.get("ensemble_rows" if arith == "exact"
+                                                    else f"ensemble_rows_{arith}"),
+                   "arithmetic": arith,
                    "parallelism": f"scenario shards x{world}"},
         "sequential_single_grid": {"value": cells / (seq_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
                                    "ms": seq_ms},
