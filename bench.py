@@ -291,8 +291,10 @@ def time_single_grid(sc, args, dev, arithmetic, clocks=None):
     if args.rows > 0:
         tuning, rows = {}, args.rows
     else:
+        # tile height timed on this very shape (cached per device), as the
+        # device loop of SWE2D.forward picks it
         tuning = autotune.tune(dev, arithmetic=arithmetic)
-        rows = autotune.tuned_rows(cells, dev, arithmetic)
+        rows = autotune.tuned_rows_for_shape(1, ny, nx, dev, arithmetic=arithmetic)
     lib = nat.lib()
     nat.check(lib.swe_tune_sweep_rows(rows), "tuned rows")
     p = nat.params(cfg, sc.dx, sc.dy, arithmetic)
