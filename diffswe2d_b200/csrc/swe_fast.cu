@@ -26,8 +26,6 @@
 // steps of the runup case, every field within 1.5x the reference's own
 // FP32-vs-FP64 difference of the FP64 reference, identical wet/dry masks.
 #include <cuda_runtime.h>
-#include <stdlib.h>
-#include <string.h>
 
 #include "swe_ensemble.cuh"
 #include "swe_sweep.cuh"
@@ -280,7 +278,7 @@ __device__ __forceinline__ State ffriction(State s, float n, float dt, const Swe
 // and cell values of row k-2, the y-face above row k-2 and the x-part of
 // row k-2's tendency; it forms row k-1's y-sides, the y-face between rows
 // k-2 and k-1, writes row k-2, and forms row k-1's x-faces.
-template <int STAGE, int FRIC, bool CG, bool U2>
+template <int STAGE, int FRIC, bool CG>
 __device__ __forceinline__ void fast_tile(const StepArgs& a, int bx, int by, int b, int rows) {
     const SweConsts& kc = a.kc;
     const int lane = threadIdx.x & 31;
@@ -324,7 +322,6 @@ __device__ __forceinline__ void fast_tile(const StepArgs& a, int bx, int by, int
     float rxA0 = 0.0f, rxA1 = 0.0f, rxA2 = 0.0f;  // x-part of row k-2's tendency
     uint32_t axb = 0u, ayb = 0u;
     bool bad = false;
-#pragma unroll(U2 ? 2 : 1)
     for (int kk = j0 - 2, it = 0; kk < jend + 2; ++kk, ++it) {
         // ---- row kk: state (predictor on stage 2) and primitives
         float s0, s1, s2, z;
@@ -435,92 +432,54 @@ __device__ __forceinline__ void fast_tile(const StepArgs& a, int bx, int by, int
     }
 }
 
-template <int STAGE, int FRIC, bool U2>
+template <int STAGE, int FRIC>
 __global__ void __launch_bounds__(SW_WARPS * 32, 8) fast_kernel(const StepArgs a) {
-    fast_tile<STAGE, FRIC, false, U2>(a, blockIdx.x, blockIdx.y, blockIdx.z, a.rows);
+    fast_tile<STAGE, FRIC, false>(a, blockIdx.x, blockIdx.y, blockIdx.z, a.rows);
 }
 
-template <bool U2>
 struct FastTile {
     template <int STAGE, int FRIC>
     static __device__ __forceinline__ void run(const StepArgs& a, int bx, int by, int rows) {
-        fast_tile<STAGE, FRIC, true, U2>(a, bx, by, 0, rows);
+        fast_tile<STAGE, FRIC, true>(a, bx, by, 0, rows);
     }
 };
 
-template <int FRIC, bool U2>
+template <int FRIC>
 __global__ void __launch_bounds__(SW_WARPS * 32, 6)
 fast_ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, EnsGlobal* g,
                      unsigned long long stall_ns) {
-    ensemble_body<FRIC, FastTile<U2>>(args, ctl, count, g, stall_ns);
-}
-
-}  // namespace
-
-namespace {
-
-// Row loop of the tolerance-mode tile unrolled by two (SWE_FAST_UNROLL=2) or
-// not (read once per process).
-bool use_unrolled_tile() {
-    static const bool unrolled = [] {
-        const char* v = getenv("SWE_FAST_UNROLL");
-        return v != nullptr && strcmp(v, "2") == 0;
-    }();
-    return unrolled;
-}
-
-template <bool U2>
-void launch_fast(int stage, const StepArgs& a, dim3 grid, cudaStream_t s) {
-    const int threads = SW_WARPS * 32;
-    if (stage & 1) fast_kernel<1, 0, U2><<<grid, threads, 0, s>>>(a);
-    if (stage & 2) {
-        if (!a.friction) fast_kernel<2, 0, U2><<<grid, threads, 0, s>>>(a);
-        else if (a.friction_model == 0) fast_kernel<2, 1, U2><<<grid, threads, 0, s>>>(a);
-        else fast_kernel<2, 2, U2><<<grid, threads, 0, s>>>(a);
-    }
+    ensemble_body<FRIC, FastTile>(args, ctl, count, g, stall_ns);
 }
 
 }  // namespace
 
 int fast_launch_stages(int stage, const StepArgs& a, dim3 grid, cudaStream_t s) {
-    if (use_unrolled_tile()) launch_fast<true>(stage, a, grid, s);
-    else launch_fast<false>(stage, a, grid, s);
+    const int threads = SW_WARPS * 32;
+    if (stage & 1) fast_kernel<1, 0><<<grid, threads, 0, s>>>(a);
+    if (stage & 2) {
+        if (!a.friction) fast_kernel<2, 0><<<grid, threads, 0, s>>>(a);
+        else if (a.friction_model == 0) fast_kernel<2, 1><<<grid, threads, 0, s>>>(a);
+        else fast_kernel<2, 2><<<grid, threads, 0, s>>>(a);
+    }
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
-namespace {
-template <bool U2>
-void launch_fast_ensemble(int friction, int blocks, const StepArgs* args, EnsCtl* ctl, int count,
-                          EnsGlobal* g, unsigned long long stall_ns, cudaStream_t s) {
-    const int threads = SW_WARPS * 32;
-    if (friction == 0)
-        fast_ensemble_kernel<0, U2><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
-    else if (friction == 1)
-        fast_ensemble_kernel<1, U2><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
-    else
-        fast_ensemble_kernel<2, U2><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
-}
-}  // namespace
-
-// The ensemble uses the same tile form as the single-grid kernels, so a
-// member's result equals the single-grid step's bit for bit.
 int fast_launch_ensemble(int friction, int blocks, const StepArgs* args, EnsCtl* ctl, int count,
                          EnsGlobal* g, unsigned long long stall_ns, cudaStream_t s) {
-    if (use_unrolled_tile()) launch_fast_ensemble<true>(friction, blocks, args, ctl, count, g, stall_ns, s);
-    else launch_fast_ensemble<false>(friction, blocks, args, ctl, count, g, stall_ns, s);
+    const int threads = SW_WARPS * 32;
+    if (friction == 0) fast_ensemble_kernel<0><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
+    else if (friction == 1) fast_ensemble_kernel<1><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
+    else fast_ensemble_kernel<2><<<blocks, threads, 0, s>>>(args, ctl, count, g, stall_ns);
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 int fast_load_kernels() {
     cudaFuncAttributes at;
     const void* fns[] = {
-        (const void*)fast_kernel<1, 0, false>, (const void*)fast_kernel<2, 0, false>,
-        (const void*)fast_kernel<2, 1, false>, (const void*)fast_kernel<2, 2, false>,
-        (const void*)fast_kernel<1, 0, true>,  (const void*)fast_kernel<2, 0, true>,
-        (const void*)fast_kernel<2, 1, true>,  (const void*)fast_kernel<2, 2, true>,
-        (const void*)fast_ensemble_kernel<0, false>, (const void*)fast_ensemble_kernel<1, false>,
-        (const void*)fast_ensemble_kernel<2, false>, (const void*)fast_ensemble_kernel<0, true>,
-        (const void*)fast_ensemble_kernel<1, true>,  (const void*)fast_ensemble_kernel<2, true>,
+        (const void*)fast_kernel<1, 0>,       (const void*)fast_kernel<2, 0>,
+        (const void*)fast_kernel<2, 1>,       (const void*)fast_kernel<2, 2>,
+        (const void*)fast_ensemble_kernel<0>, (const void*)fast_ensemble_kernel<1>,
+        (const void*)fast_ensemble_kernel<2>,
     };
     for (const void* f : fns)
         if (cudaFuncGetAttributes(&at, f) != cudaSuccess) return SWE_ECUDA;
