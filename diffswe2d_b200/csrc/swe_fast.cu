@@ -119,10 +119,13 @@ __device__ __forceinline__ FDiff fdiff(const FPrim& hi, const FPrim& lo) {
 }
 
 // Half of limited_increment (numerics.py:4-27) from the backward and forward
-// differences: 0.5 minmod3(theta b, (b+f)/2, theta f).
+// differences: 0.5 minmod3(theta b, (b+f)/2, theta f).  minmod3 of values
+// whose minimum is lo and maximum hi is max(lo, min(hi, 0)).
 __device__ __forceinline__ float half_inc(float b, float f, const FK& k) {
     const float x = k.ht * b, y = k.ht * f, c = 0.25f * (b + f);
-    return fmaxf(min3f(x, c, y), 0.0f) + fminf(max3f(x, c, y), 0.0f);
+    // the median of (min, 0, max): the minimum if all three are positive,
+    // the maximum if all are negative, else 0
+    return fmaxf(min3f(x, c, y), fminf(max3f(x, c, y), 0.0f));
 }
 
 struct FSide {
@@ -182,19 +185,22 @@ __device__ __forceinline__ FFace fface(const FSide& L, float hLc, float zLc, con
     const float hR = fmaxf(fminf(R.eta - bcn, R.hlin), 0.0f);
     const float srcL = k.half_g * (hLc + hL) * (zLc - bcn);
     const float srcR = k.half_g * (hR + hRc) * (zRc - bcn);
-    // primitive() of the face states: (h u)/max(h, floor) is u when h >= floor
+    // primitive() of the face states: (h u)/max(h, floor) is u min(h/floor, 1)
+    // on wet states and 0 on dry ones -- a mask multiplied in (1 or 0, with
+    // the floor's factor when the floor exceeds the dry depth)
     const bool wL = hL > k.dry, wR = hR > k.dry;
-    float sL = 1.0f, sR = 1.0f;
+    const float wmL = wL ? 1.0f : 0.0f, wmR = wR ? 1.0f : 0.0f;
+    float mL = wmL, mR = wmR;
     if (k.floor_above_dry) {
-        sL = fminf(hL * k.rfloor, 1.0f);
-        sR = fminf(hR * k.rfloor, 1.0f);
+        mL *= fminf(hL * k.rfloor, 1.0f);
+        mR *= fminf(hR * k.rfloor, 1.0f);
     }
-    const float unL = wL ? (NY ? L.v : L.u) * sL : 0.0f;
-    const float utL = wL ? (NY ? L.u : L.v) * sL : 0.0f;
-    const float unR = wR ? (NY ? R.v : R.u) * sR : 0.0f;
-    const float utR = wR ? (NY ? R.u : R.v) * sR : 0.0f;
-    const float cL = wL ? sqrta(k.g * fmaxf(hL, k.floor_h)) : 0.0f;
-    const float cR = wR ? sqrta(k.g * fmaxf(hR, k.floor_h)) : 0.0f;
+    const float unL = (NY ? L.v : L.u) * mL;
+    const float utL = (NY ? L.u : L.v) * mL;
+    const float unR = (NY ? R.v : R.u) * mR;
+    const float utR = (NY ? R.u : R.v) * mR;
+    const float cL = sqrta(k.g * fmaxf(hL, k.floor_h)) * wmL;
+    const float cR = sqrta(k.g * fmaxf(hR, k.floor_h)) * wmR;
     const float us = 0.5f * (unL + unR) + cL - cR;
     const float cs = 0.5f * (cL + cR) + 0.25f * (unL - unR);
     const float SL = wL ? fminf(unL - cL, us - cs) : unR - 2.0f * cR;
