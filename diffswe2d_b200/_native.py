@@ -158,6 +158,8 @@ _SIGNATURES = {
                             _P, _P, _I, _P],
     "swe_adj_spatial_bed_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _P,
                                 _P, _P, _P, _I, _P, _P],
+    "swe_adj_stage2_f32": [_P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P,
+                           _P, _P, _F, _P, _P, _P, _P, _I, _P, _P],
     "swe_adj_pointwise_f32": [_I, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _F, _P,
                               _P, _P, _P, _P, _P],
     "swe_adj_pointwise_dev_f32": [_I, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P,

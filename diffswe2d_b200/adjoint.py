@@ -50,7 +50,6 @@ class AdjointStepper:
         rec = 16 if self.bed_grad else 12  # floats per face record
         self.K1, self.K2, self.P = (torch.empty(shape, device=dev) for _ in range(3))
         self.lam_k = torch.empty(shape, device=dev)
-        self.lam_P = torch.empty(shape, device=dev)
         self.red = torch.empty(nat.RED_WORDS, dtype=torch.int32, device=dev)
         self.cx = torch.empty(B * ny * (nx + 1) * rec, device=dev)
         self.cy = torch.empty(B * (ny + 1) * nx * rec, device=dev)
@@ -88,6 +87,19 @@ class AdjointStepper:
             rc = self.lib.swe_adj_spatial_f32(*args, self.st)
         nat.check(rc, what)
 
+    def _stage2(self, P, U, K1, lv, dt, lam_U):
+        """Spatial adjoint at the predictor P (lam_rhs = self.lam_k, the
+        adjoint of k2) and the predictor's adjoint in one call: lam_U += ...,
+        self.lam_k = adjoint of k1 (written after the last read of k2's)."""
+        dev_dt = torch.is_tensor(dt)
+        rc = self.lib.swe_adj_stage2_f32(
+            nat.ptr(P), nat.ptr(U), nat.ptr(K1), nat.ptr(self.bed), self.bed.shape[0], self.B, self.ny,
+            self.nx, self.p, nat.ptr(lv), self.levelB, nat.ptr(self.lam_k), nat.ptr(self.cx),
+            nat.ptr(self.cy), 0.0 if dev_dt else float(dt), nat.ptr(dt) if dev_dt else None,
+            nat.ptr(lam_U), nat.ptr(self.lam_k), nat.ptr(self.part[0]), LEVEL_BLOCKS,
+            nat.ptr(self.lam_bed) if self.bed_grad else None, self.st)
+        nat.check(rc, "adjoint spatial operator and predictor (stage 2)")
+
     def bed_adjoint(self):
         """The accumulated bed adjoint in the bed's batch form
         [bedB, 1, ny, nx] (summed over the batch for a shared bed)."""
@@ -120,21 +132,17 @@ class AdjointStepper:
         [2, B * LEVEL_BLOCKS] (their sum per batch member is that member's
         level adjoint).  K1, if given, is the step's stage-1 tendency kept
         from the forward recompute (else it is recomputed here)."""
-        lib, st, p, B, ny, nx = self.lib, self.st, self.p, self.B, self.ny, self.nx
-        K2, P, lam_k, lam_P = self.K2, self.P, self.lam_k, self.lam_P
+        K2, P, lam_k = self.K2, self.P, self.lam_k
         # recompute the step's stage intermediates (solver.py:613-646)
         if K1 is None:
             K1 = self.K1
             self._tendency(U, lv, K1)
         self._pointwise(2, U, K1, dt, None, None, None, P)
         self._tendency(P, lv, K2)
-        lam_P.zero_()
-        # corrector + friction
+        # corrector + friction: lam_k = adjoint of k2
         self._pointwise(0, U, K2, dt, lam_out, lam_U, lam_n, None)
-        # spatial operator at the predictor
-        self._spatial(P, lv, lam_k, lam_P, self.part[0], "adjoint spatial operator (stage 2)")
-        # predictor
-        self._pointwise(1, U, K1, dt, lam_P, lam_U, None, None)
+        # spatial operator at the predictor, then the predictor: lam_k = adjoint of k1
+        self._stage2(P, U, K1, lv, dt, lam_U)
         # spatial operator at the input state
         self._spatial(U, lv, lam_k, lam_U, self.part[1], "adjoint spatial operator (stage 1)")
         return self.part

@@ -6,557 +6,37 @@
 // Q = C(U, U + dt k2), U' = F(Q, n).  Its adjoint runs, per step:
 //   swe_adj_pointwise_f32(mode 0): friction and corrector clean-up adjoints
 //       (friction.py:12-131, solver.py:547-570) -> lamU, lam_k2, lam_n
-//   swe_adj_spatial_f32 on P:     adjoint of the spatial operator -> lam_P
-//   swe_adj_pointwise_f32(mode 1): predictor clean-up adjoint -> lamU, lam_k1
-//   swe_adj_spatial_f32 on U:     -> lamU
-// The spatial-operator adjoint is two kernels: one thread per face computes
-// the face's reverse mode (swe_adjoint.cuh) and writes its contributions to
-// its four stencil cells into a face-indexed buffer; one thread per cell then
-// sums them in a fixed order and folds the adjoints of ghost cells back into
-// the interior cells and boundary level they were made from (the adjoint of
-// add_ghost_cells, src/boundary.py:150-413).  No float atomics: results are
-// deterministic.
-#include <cuda_runtime.h>
-#include <stdint.h>
-
-#include "swe_adjoint.cuh"
-#include "swe_common.cuh"
-
-namespace swe {
-namespace {
-
-constexpr int ADJ_THREADS = 256;
-// The face and gather kernels are latency-bound at low occupancy; three
-// blocks per SM (80 / 72 registers, a few hundred bytes of spills in the
-// face kernel) measured 2.5-9 % faster per inversion iteration than two.
-
-struct AdjArgs {
-    const float* S;      // state whose tendency is differentiated, [B,3,ny,nx]
-    const float* bed;    // [bedB,1,ny,nx]
-    const float* level;  // [levelB]
-    const float* lrhs;   // adjoint of the tendency, [B,3,ny,nx]
-    float* cx;           // x-face contributions [B][ny][nx+1][12]
-    float* cy;           // y-face contributions [B][ny+1][nx][12]
-    float* lS;           // adjoint of S, accumulated (+=)
-    float* llevel_part;  // per-block partial level adjoints [B][gridDim.x]
-    float* lbed;         // adjoint of the bed [B,ny,nx], accumulated (+=); BEDG only
-    int B, bedB, levelB, ny, nx;
-    int bc[4];
-    float cval;
-    int wsr;
-    SweConsts kc;
-};
-
-__device__ __forceinline__ size_t a3(int b, int c, int j, int i, int ny, int nx) {
-    return (((size_t)b * 3 + c) * ny + j) * nx + i;
-}
-
-__device__ __forceinline__ float bed_of(const AdjArgs& a, int b, int j, int i) {
-    return a.bed[((size_t)(a.bedB == 1 ? 0 : b) * a.ny + j) * a.nx + i];
-}
-
-// Padded cell (j, i) of S with the ghost rules (arm cells only; corners are
-// never part of an interior face's stencil).
-__device__ PrimRec padded_prim(const AdjArgs& a, int b, int j, int i) {
-    const int ny = a.ny, nx = a.nx;
-    const bool jin = (unsigned)j < (unsigned)ny, iin = (unsigned)i < (unsigned)nx;
-    int js = min(max(j, 0), ny - 1), is = min(max(i, 0), nx - 1);
-    const bool xarm = jin && !iin, yarm = iin && !jin;
-    int code = -1, side = 0;
-    if (xarm || yarm) {
-        side = xarm ? (i < 0 ? 0 : 1) : (j < 0 ? 2 : 3);
-        code = a.bc[side];
-        if (code == SWE_BC_PERIODIC) {
-            if (xarm) is = i < 0 ? nx + i : i - nx;
-            else js = j < 0 ? ny + j : j - ny;
-        }
-    }
-    const size_t plane = (size_t)ny * nx;
-    const size_t o = a3(b, 0, js, is, ny, nx);
-    float U0 = a.S[o], U1 = a.S[o + plane], U2 = a.S[o + 2 * plane];
-    const float z = bed_of(a, b, js, is);
-    const float lev = a.level[a.levelB == 1 ? 0 : b];
-    if (code == SWE_BC_CONSTANT) {
-        U0 = U1 = U2 = a.cval;
-    } else if (code == SWE_BC_WATER_LEVEL) {
-        U0 = fmaxf(lev - z, 0.0f);
-    } else if (code == SWE_BC_WALL) {
-        const int jm = xarm ? j : (j < 0 ? -1 - j : 2 * ny - 1 - j);
-        const int im = xarm ? (i < 0 ? -1 - i : 2 * nx - 1 - i) : i;
-        const size_t om = a3(b, xarm ? 1 : 2, jm, im, ny, nx);
-        if (xarm) U1 = -a.S[om];
-        else U2 = -a.S[om];
-    } else if (code == SWE_BC_ABSORBING) {
-        const float hr = fmaxf(lev - z, 0.0f);
-        const float hg = U0;
-        const float hc = hr > a.kc.absorb_lim ? hr : hg;
-        const float c = root(a.kc.g981 * fmaxf(hc, a.kc.absorb_min));
-        const float val = ((side == 0 || side == 2) ? -c : c) * (hg - hr);
-        if (xarm) U1 = val;
-        else U2 = val;
-    }
-    return prim_rec(U0, U1, U2, z, a.kc);
-}
-
-// Face records: 4 cells x (U0, U1, U2[, Z]) floats.
-template <bool BEDG>
-__host__ __device__ constexpr int rec_floats() { return BEDG ? 16 : 12; }
-
-template <bool DIRY, bool BEDG>
-__global__ void __launch_bounds__(ADJ_THREADS, 3) adj_face_kernel(const AdjArgs a) {
-    const int ny = a.ny, nx = a.nx;
-    const long long nfaces = DIRY ? (long long)(ny + 1) * nx : (long long)ny * (nx + 1);
-    const long long total = nfaces * a.B;
-    const size_t plane = (size_t)ny * nx;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int b = (int)(t / nfaces);
-        const long long r = t - (long long)b * nfaces;
-        int row, f;  // x: row j, face f in [0, nx]; y: face f in [0, ny], column i (row var)
-        if (DIRY) {
-            f = (int)(r / nx);
-            row = (int)(r - (long long)f * nx);
-        } else {
-            row = (int)(r / (nx + 1));
-            f = (int)(r - (long long)row * (nx + 1));
-        }
-        PrimRec P[4];
-        for (int s = 0; s < 4; ++s) P[s] = DIRY ? padded_prim(a, b, f - 2 + s, row) : padded_prim(a, b, row, f - 2 + s);
-        // adjoints of the face outputs from the tendencies of the two cells
-        // sharing the face: (F_right(f) - F_left(f+1)) / d
-        const float d = DIRY ? a.kc.dy : a.kc.dx;
-        const float rd = DIRY ? a.kc.rdy : a.kc.rdx;  // RN(1/d): lrhs / d below is exact RN
-        const int n = DIRY ? ny : nx;
-        float r0p = 0.0f, r1p = 0.0f, r2p = 0.0f, r0m = 0.0f, r1m = 0.0f, r2m = 0.0f;
-        if (f < n) {  // cell f: this face is its left/top face
-            const size_t o = DIRY ? a3(b, 0, f, row, ny, nx) : a3(b, 0, row, f, ny, nx);
-            r0p = quot(a.lrhs[o], d, rd);
-            r1p = quot(a.lrhs[o + plane], d, rd);
-            r2p = quot(a.lrhs[o + 2 * plane], d, rd);
-        }
-        if (f >= 1) {  // cell f-1: this face is its right/bottom face
-            const size_t o = DIRY ? a3(b, 0, f - 1, row, ny, nx) : a3(b, 0, row, f - 1, ny, nx);
-            r0m = quot(a.lrhs[o], d, rd);
-            r1m = quot(a.lrhs[o + plane], d, rd);
-            r2m = quot(a.lrhs[o + 2 * plane], d, rd);
-        }
-        const float l_mass = r0p - r0m;
-        // x: channel 1 normal, 2 tangential; y: channel 1 tangential, 2 normal
-        const float l_nR = DIRY ? r2p : r1p;
-        const float l_nL = DIRY ? -r2m : -r1m;
-        const float l_tan = DIRY ? (r1p - r1m) : (r2p - r2m);
-        CellAdj out[4];
-        face_vjp<BEDG>(P, l_mass, l_nL, l_nR, l_tan, DIRY, a.kc, a.wsr != 0, out);
-        constexpr int C = BEDG ? 4 : 3;
-        float* dst = (DIRY ? a.cy : a.cx) + (size_t)t * rec_floats<BEDG>();
-        for (int s = 0; s < 4; ++s) {
-            dst[C * s] = out[s].U0;
-            dst[C * s + 1] = out[s].U1;
-            dst[C * s + 2] = out[s].U2;
-            if (BEDG) dst[C * s + 3] = out[s].Z;
-        }
-    }
-}
-
-// Sum of the face contributions to padded cell (row j, column col) along x
-// (l[3], the bed channel, with BEDG only).
-template <bool BEDG>
-__device__ void lam_x(const AdjArgs& a, int b, int j, int col, float l[4]) {
-    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
-    l[0] = l[1] = l[2] = l[3] = 0.0f;
-    for (int f = col - 1; f <= col + 2; ++f) {
-        if (f < 0 || f > a.nx) continue;
-        const float* c = a.cx + ((((size_t)b * a.ny + j) * (a.nx + 1) + f) * R) + C * (col - f + 2);
-        l[0] += c[0];
-        l[1] += c[1];
-        l[2] += c[2];
-        if (BEDG) l[3] += c[3];
-    }
-}
-
-template <bool BEDG>
-__device__ void lam_y(const AdjArgs& a, int b, int row, int i, float l[4]) {
-    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
-    l[0] = l[1] = l[2] = l[3] = 0.0f;
-    for (int f = row - 1; f <= row + 2; ++f) {
-        if (f < 0 || f > a.ny) continue;
-        const float* c = a.cy + ((((size_t)b * (a.ny + 1) + f) * a.nx + i) * R) + C * (row - f + 2);
-        l[0] += c[0];
-        l[1] += c[1];
-        l[2] += c[2];
-        if (BEDG) l[3] += c[3];
-    }
-}
-
-// Folds the adjoint lg of ghost g (side `side`; g its column for left/right,
-// row for top/bottom) into cell (j, i) if the ghost was made from it, and
-// adds the level adjoint once per ghost (in the thread of the ghost's
-// clamped source cell).  BEDG: lg[3] is the ghost's bed adjoint, folded into
-// the cell its bed was copied from (replicate, or periodic), plus the bed
-// terms of the forced ghost depth max(level - z, 0) -> lzc.
-template <bool BEDG>
-__device__ void fold_ghost(const AdjArgs& a, int b, int side, int g, const float lg[4], int j,
-                           int i, float lam[3], float& llev, float& lzc) {
-    const int ny = a.ny, nx = a.nx;
-    const bool xs = side < 2;
-    const int n = xs ? nx : ny;
-    const int pos = xs ? i : j;  // this cell's index along the side's direction
-    const int clamp_src = g < 0 ? 0 : n - 1;
-    const int mirror = g < 0 ? -1 - g : 2 * n - 1 - g;
-    const int periodic = g < 0 ? n + g : g - n;
-    const int normal = xs ? 1 : 2;  // momentum channel reflected by a wall
-    const int code = a.bc[side];
-    if (BEDG && pos == (code == SWE_BC_PERIODIC ? periodic : clamp_src)) lzc += lg[3];
-    switch (code) {
-    case SWE_BC_TRANSMISSIVE:
-        if (pos == clamp_src) {
-            lam[0] += lg[0];
-            lam[1] += lg[1];
-            lam[2] += lg[2];
-        }
-        break;
-    case SWE_BC_PERIODIC:
-        if (pos == periodic) {
-            lam[0] += lg[0];
-            lam[1] += lg[1];
-            lam[2] += lg[2];
-        }
-        break;
-    case SWE_BC_CONSTANT:
-        break;
-    case SWE_BC_WATER_LEVEL:
-        if (pos == clamp_src) {
-            lam[1] += lg[1];
-            lam[2] += lg[2];
-            const float z = bed_of(a, b, xs ? j : clamp_src, xs ? clamp_src : i);
-            const float lev = a.level[a.levelB == 1 ? 0 : b];
-            if (lev - z >= 0.0f) {  // clamp(level - z, min=0)
-                llev += lg[0];
-                if (BEDG) lzc -= lg[0];
-            }
-        }
-        break;
-    case SWE_BC_WALL:
-        if (pos == clamp_src) {
-            lam[0] += lg[0];
-            lam[3 - normal] += lg[3 - normal];
-        }
-        if (pos == mirror) lam[normal] -= lg[normal];
-        break;
-    case SWE_BC_ABSORBING:
-        if (pos == clamp_src) {
-            lam[3 - normal] += lg[3 - normal];
-            lam[0] += lg[0];
-            // value = s c (hg - hr), hr = max(level - z, 0),
-            // c = sqrt(9.81 max(where(hr > 1e-4, hr, hg), 1e-6))
-            const size_t plane = (size_t)ny * nx;
-            const int jj = xs ? j : clamp_src, ii = xs ? clamp_src : i;
-            const float hg = a.S[a3(b, 0, jj, ii, ny, nx)];
-            (void)plane;
-            const float z = bed_of(a, b, jj, ii);
-            const float lev = a.level[a.levelB == 1 ? 0 : b];
-            const float hr = fmaxf(lev - z, 0.0f);
-            const bool use_hr = hr > a.kc.absorb_lim;
-            const float hc = use_hr ? hr : hg;
-            const float cm = fmaxf(hc, a.kc.absorb_min);
-            const float c = root(a.kc.g981 * cm);
-            const float s = (side == 0 || side == 2) ? -1.0f : 1.0f;
-            const float lv = lg[normal];
-            const float l_c = lv * (s * (hg - hr));
-            const float l_diff = lv * (s * c);
-            float l_hc = 0.0f;
-            if (hc >= a.kc.absorb_min) {
-                const float c2 = 2.0f * c;
-                l_hc = a.kc.g981 * quot(l_c, c2, shared_rcp(c2));
-            }
-            float l_hg = l_diff + (use_hr ? 0.0f : l_hc);
-            float l_hr = -l_diff + (use_hr ? l_hc : 0.0f);
-            lam[0] += l_hg;
-            if (lev - z >= 0.0f) {
-                llev += l_hr;
-                if (BEDG) lzc -= l_hr;
-            }
-        }
-        break;
-    default:
-        break;
-    }
-}
-
-template <bool BEDG>
-__global__ void __launch_bounds__(ADJ_THREADS, 3) adj_gather_kernel(const AdjArgs a) {
-    const int ny = a.ny, nx = a.nx;
-    const int b = blockIdx.y;
-    const long long ncell = (long long)ny * nx;
-    const size_t plane = (size_t)ny * nx;
-    float llev = 0.0f;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(t / nx), i = (int)(t - (long long)(t / nx) * nx);
-        float lam[4], l[4];
-        lam_x<BEDG>(a, b, j, i, lam);
-        lam_y<BEDG>(a, b, j, i, l);
-        lam[0] += l[0];
-        lam[1] += l[1];
-        lam[2] += l[2];
-        float lz = BEDG ? lam[3] + l[3] : 0.0f;
-        if (i < 2 || i >= nx - 2) {
-            const int gx[4] = {-1, -2, nx, nx + 1};
-            for (int q = 0; q < 4; ++q) {
-                lam_x<BEDG>(a, b, j, gx[q], l);
-                fold_ghost<BEDG>(a, b, q < 2 ? 0 : 1, gx[q], l, j, i, lam, llev, lz);
-            }
-        }
-        if (j < 2 || j >= ny - 2) {
-            const int gy[4] = {-1, -2, ny, ny + 1};
-            for (int q = 0; q < 4; ++q) {
-                lam_y<BEDG>(a, b, gy[q], i, l);
-                fold_ghost<BEDG>(a, b, q < 2 ? 2 : 3, gy[q], l, j, i, lam, llev, lz);
-            }
-        }
-        const size_t o = a3(b, 0, j, i, ny, nx);
-        a.lS[o] += lam[0];
-        a.lS[o + plane] += lam[1];
-        a.lS[o + 2 * plane] += lam[2];
-        if (BEDG) a.lbed[(size_t)b * plane + (size_t)j * nx + i] += lz;
-    }
-    // per-block partial sum of the level adjoint (fixed order)
-    __shared__ float s_part[ADJ_THREADS / 32];
-    for (int off = 16; off > 0; off >>= 1) llev += __shfl_down_sync(0xffffffffu, llev, off);
-    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = llev;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float sum = 0.0f;
-        for (int w = 0; w < ADJ_THREADS / 32; ++w) sum += s_part[w];
-        a.llevel_part[(size_t)b * gridDim.x + blockIdx.x] = sum;
-    }
-}
-
-// ------------------------------------------------------- pointwise adjoints
-struct PwArgs {
-    const float* U;     // step input
-    const float* k;     // tendency (k2 for mode 0, k1 for mode 1)
-    const float* n;     // roughness (mode 0)
-    const float* lout;  // adjoint of the step output (mode 0) or of P (mode 1)
-    float* lU;          // adjoint of U, accumulated (+=)
-    float* lk;          // adjoint of the tendency (written)
-    float* ln;          // adjoint of the roughness field, accumulated (+=) [nB,ny,nx]
-    float* P;           // mode 2: predictor output
-    float scale;        // dt (mode 0) or dt/2 (modes 1, 2)
-    float dt;
-    const float* dt_dev;  // if set: dt read from device memory (scale derived here)
-    int B, nB, ny, nx, mode, positivity, friction, friction_model;
-    SweConsts kc;
-};
-
-// Adjoint of _clean_and_limit (solver.py:547-570): returns lam_old, lam_cand.
-__device__ void clean_bwd(const State& o, const State& c, const State& lout, const SweConsts& k,
-                          bool positivity, State& lold, State& lcand) {
-    State cp = c;
-    float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, th = 1.0f, ratio = 0.0f, safe = 0.0f, ysafe = 0.0f;
-    bool theta_branch = false;
-    if (positivity) {
-        d0 = c.h - o.h;
-        d1 = c.hu - o.hu;
-        d2 = c.hv - o.hv;
-        safe = fmaxf(-d0, k.eps);
-        ysafe = shared_rcp(safe);
-        ratio = quot(o.h, safe, ysafe);
-        theta_branch = d0 < 0.0f;
-        th = theta_branch ? fminf(ratio, 1.0f) : 1.0f;
-        cp.h = o.h + th * d0;
-        cp.hu = o.hu + th * d1;
-        cp.hv = o.hv + th * d2;
-    }
-    const float h = fmaxf(cp.h, 0.0f);
-    const bool wet = h > k.dry;
-    State lcp;
-    lcp.h = cp.h >= 0.0f ? lout.h : 0.0f;
-    lcp.hu = wet ? lout.hu : 0.0f;
-    lcp.hv = wet ? lout.hv : 0.0f;
-    if (!positivity) {
-        lold = State{0.0f, 0.0f, 0.0f};
-        lcand = lcp;
-        return;
-    }
-    // cand' = old + th * delta
-    const float l_th = lcp.h * d0 + lcp.hu * d1 + lcp.hv * d2;
-    float ld0 = lcp.h * th, ld1 = lcp.hu * th, ld2 = lcp.hv * th;
-    lold = lcp;
-    if (theta_branch && ratio <= 1.0f) {  // th = clamp(old_h / safe, max=1)
-        lold.h += quot(l_th, safe, ysafe);
-        const float l_safe = -l_th * quot(ratio, safe, ysafe);
-        if (-d0 >= k.eps) ld0 -= l_safe;  // safe = clamp(-dh, min=eps)
-    }
-    lcand = State{ld0, ld1, ld2};
-    lold.h -= ld0;
-    lold.hu -= ld1;
-    lold.hv -= ld2;
-}
-
-// Adjoint of the friction update (friction.py:12-131) w.r.t. its input state
-// and the roughness field.
-__device__ void friction_bwd(const State& s0, float n, float dt, int model, const SweConsts& k,
-                             const State& lout, State& ls, float& ln) {
-    const float h = fmaxf(s0.h, 0.0f);
-    const bool wet = h > k.dry;
-    const float safe = fmaxf(h, k.fr_vs);
-    const float ys = shared_rcp(safe);
-    const float u = quot(wet ? s0.hu : 0.0f, safe, ys), v = quot(wet ? s0.hv : 0.0f, safe, ys);
-    const float sp2 = u * u + v * v;
-    const bool moving = wet && sp2 > 0.0f;
-    const float S = fmaxf(sp2, k.fr_e2);
-    const float speed = moving ? root(S) : 0.0f;
-    float cf;
-    // cf and d cf / d h, d cf / d n (as autograd evaluates them)
-    float dcf_dpre = 0.0f, dcf_dn = 0.0f, hpre = 0.0f;
-    bool h_pass = false, n_pass = false;
-    if (model == 0) {
-        const float nn = fmaxf(n, 0.0f);
-        hpre = fmaxf(h, k.fr_e);
-        const float pw = pow_third(hpre, k.third);
-        const float num = k.g981 * (nn * nn);
-        const float ypw = shared_rcp(pw);
-        cf = quot(num, pw, ypw);
-        // d/d pw: -cf / pw ; d pw / d hpre = third * hpre^(third - 1)
-        const float dpw = k.third * pow_pos(hpre, k.third - 1.0f);
-        dcf_dpre = -quot(cf, pw, ypw) * dpw;
-        dcf_dn = quot(k.g981 * (2.0f * nn), pw, ypw);
-        h_pass = h >= k.fr_e;
-        n_pass = n >= 0.0f;
-    } else {
-        const float zz = fmaxf(n, k.fr_e);
-        hpre = fmaxf(h, k.fr_e);
-        const float yzz = shared_rcp(zz);
-        const float ratio = quot(hpre, zz, yzz);
-        const float shallow_den = fmaxf(0.46f * ratio, k.fr_e);
-        const float rc = fmaxf(ratio, k.fr_e);
-        const float lg = (float)log((double)rc);
-        const float inv_rc = recip(rc);
-        const float lt = 2.5f * ((lg - 1.0f) + inv_rc * 1.359f);
-        const float deep_den = fmaxf(lt * lt, k.fr_e);
-        const bool shallow_b = ratio < 2.71828182845904523536f;
-        cf = shallow_b ? recip(shallow_den) : recip(deep_den);
-        float dcf_dratio;
-        if (shallow_b) {
-            dcf_dratio = (0.46f * ratio >= k.fr_e) ? -(cf * cf) * 0.46f : 0.0f;
-        } else {
-            float dlt = 0.0f;
-            if (ratio >= k.fr_e) dlt = 2.5f * (inv_rc - 1.359f * inv_rc * inv_rc);
-            dcf_dratio = (lt * lt >= k.fr_e) ? -(cf * cf) * (2.0f * lt) * dlt : 0.0f;
-        }
-        dcf_dpre = quot(dcf_dratio, zz, yzz);
-        dcf_dn = -dcf_dratio * quot(ratio, zz, yzz);
-        h_pass = h >= k.fr_e;
-        n_pass = n >= k.fr_e;
-    }
-    const float X = quot((cf * speed) * dt, safe, ys);
-    const float fac = recip(1.0f + X);
-    ls.h = lout.h;
-    ls.hu = wet ? lout.hu * fac : 0.0f;
-    ls.hv = wet ? lout.hv * fac : 0.0f;
-    float l_fac = wet ? lout.hu * s0.hu + lout.hv * s0.hv : 0.0f;
-    const float l_D = -l_fac * (fac * fac);
-    const float l_num = quot(l_D, safe, ys);  // d/d((cf speed) dt)
-    float l_safe = -l_D * quot(X, safe, ys);
-    const float l_cs = l_num * dt;
-    const float l_cf = l_cs * speed;
-    const float l_speed = l_cs * cf;
-    float l_u = 0.0f, l_v = 0.0f;
-    if (moving) {
-        const float s2 = 2.0f * speed;
-        const float l_S = quot(l_speed, s2, shared_rcp(s2));
-        if (sp2 >= k.fr_e2) {
-            l_u = l_S * (2.0f * u);
-            l_v = l_S * (2.0f * v);
-        }
-    }
-    if (wet) {
-        ls.hu += quot(l_u, safe, ys);
-        ls.hv += quot(l_v, safe, ys);
-    }
-    l_safe -= l_u * quot(u, safe, ys) + l_v * quot(v, safe, ys);
-    float l_h = 0.0f;
-    if (h >= k.fr_vs) l_h += l_safe;
-    if (h_pass) l_h += l_cf * dcf_dpre;
-    ln = n_pass ? l_cf * dcf_dn : 0.0f;
-    if (s0.h >= 0.0f) ls.h += l_h;
-}
-
-__global__ void adj_pointwise_kernel(const PwArgs a) {
-    const long long plane = (long long)a.ny * a.nx;
-    const long long total = plane * a.B;
-    float dt = a.dt, scale = a.scale;
-    if (a.dt_dev != nullptr) {
-        dt = *a.dt_dev;
-        scale = a.mode == 0 ? dt : 0.5f * dt;
-    }
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int b = (int)(t / plane);
-        const long long i = t - (long long)b * plane;
-        const size_t o = (size_t)b * 3 * plane + i;
-        const State u{a.U[o], a.U[o + plane], a.U[o + 2 * plane]};
-        const State cand{u.h + scale * a.k[o], u.hu + scale * a.k[o + plane],
-                         u.hv + scale * a.k[o + 2 * plane]};
-        if (a.mode == 2) {  // predictor forward, solver.py:639
-            const State p = clean_and_limit(u, cand, a.kc, a.positivity != 0);
-            a.P[o] = p.h;
-            a.P[o + plane] = p.hu;
-            a.P[o + 2 * plane] = p.hv;
-            continue;
-        }
-        State lq{a.lout[o], a.lout[o + plane], a.lout[o + 2 * plane]};
-        if (a.mode == 0 && a.friction) {
-            const State q = clean_and_limit(u, cand, a.kc, a.positivity != 0);
-            const size_t on = (size_t)(a.nB == 1 ? 0 : b) * plane + i;
-            State lqi;
-            float ln = 0.0f;
-            friction_bwd(q, a.n[on], dt, a.friction_model, a.kc, lq, lqi, ln);
-            lq = lqi;
-            if (a.nB == 1 && a.B > 1) atomicAdd(&a.ln[on], ln);
-            else a.ln[on] += ln;
-        }
-        State lold, lcand;
-        clean_bwd(u, cand, lq, a.kc, a.positivity != 0, lold, lcand);
-        // cand = U + scale * k
-        a.lU[o] += lold.h + lcand.h;
-        a.lU[o + plane] += lold.hu + lcand.hu;
-        a.lU[o + 2 * plane] += lold.hv + lcand.hv;
-        a.lk[o] = lcand.h * scale;
-        a.lk[o + plane] = lcand.hu * scale;
-        a.lk[o + 2 * plane] = lcand.hv * scale;
-    }
-}
-
-int blocks_for(long long n) {
-    long long b = (n + ADJ_THREADS - 1) / ADJ_THREADS;
-    if (b < 1) b = 1;
-    return (int)(b > 148LL * 32 ? 148LL * 32 : b);
-}
-
-}  // namespace
-}  // namespace swe
+//   swe_adj_stage2_f32 at P:       adjoint of the spatial operator and of
+//       the predictor clean-up (solver.py:639) -> lamU, lam_k1
+//   swe_adj_spatial_f32 on U:      -> lamU
+// (swe_adj_stage2_f32 is swe_adj_spatial_f32 into a zeroed lam_P followed
+// by swe_adj_pointwise_f32 mode 1, in two launches instead of three.)
+// The kernels are in swe_adjoint_kernels.cuh.  This file holds the C ABI and
+// the IEEE instantiation (ExactMath, for SWE_ARITH_EXACT parameters);
+// parameters with SWE_ARITH_FAST run the FastMath instantiation of
+// swe_adjoint_fast.cu.
+#include "swe_adjoint_kernels.cuh"
 
 using namespace swe;
 
 namespace {
-int adj_spatial(const float* S, const float* bed, int bedB, int B, int ny, int nx,
-                const swe_params* p, const float* level, int levelB, const float* lam_rhs,
-                float* scratch_cx, float* scratch_cy, float* lam_S, float* level_part,
-                int level_blocks, float* lam_bed, void* stream) {
-    if (!S || !bed || !level || !lam_rhs || !scratch_cx || !scratch_cy || !lam_S || !level_part)
+
+// The spatial adjoint's arguments (checked), without the fused-predictor part.
+int adj_args(AdjArgs& a, const float* S, const float* bed, int bedB, int B, int ny, int nx,
+             const swe_params* p, const float* level, int levelB, const float* lam_rhs,
+             float* scratch_cx, float* scratch_cy, float* level_part, int level_blocks,
+             float* lam_bed) {
+    if (!S || !bed || !level || !lam_rhs || !scratch_cx || !scratch_cy || !level_part)
         return SWE_EARG;
     if (!valid_params(p) || B < 1 || ny < 2 || nx < 2 || level_blocks < 1) return SWE_EARG;
     if ((bedB != 1 && bedB != B) || (levelB != 1 && levelB != B) || B > 65535) return SWE_EARG;
-    AdjArgs a{};
+    a = AdjArgs{};
     a.S = S;
     a.bed = bed;
     a.level = level;
     a.lrhs = lam_rhs;
     a.cx = scratch_cx;
     a.cy = scratch_cy;
-    a.lS = lam_S;
     a.llevel_part = level_part;
     a.lbed = lam_bed;
     a.B = B;
@@ -571,18 +51,27 @@ int adj_spatial(const float* S, const float* bed, int bedB, int B, int ny, int n
     a.cval = (float)p->constant_value;
     a.wsr = p->water_slope_reset;
     a.kc = make_consts(*p);
+    a.positivity = p->positivity_limiter;
+    return SWE_OK;
+}
+
+int run_spatial(const AdjArgs& a, const swe_params* p, int level_blocks, bool pred, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    const int gx = blocks_for((long long)B * ny * (nx + 1)), gy = blocks_for((long long)B * (ny + 1) * nx);
-    if (lam_bed) {
-        adj_face_kernel<false, true><<<gx, ADJ_THREADS, 0, s>>>(a);
-        adj_face_kernel<true, true><<<gy, ADJ_THREADS, 0, s>>>(a);
-        adj_gather_kernel<true><<<dim3(level_blocks, B), ADJ_THREADS, 0, s>>>(a);
-    } else {
-        adj_face_kernel<false, false><<<gx, ADJ_THREADS, 0, s>>>(a);
-        adj_face_kernel<true, false><<<gy, ADJ_THREADS, 0, s>>>(a);
-        adj_gather_kernel<false><<<dim3(level_blocks, B), ADJ_THREADS, 0, s>>>(a);
-    }
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    if (p->arithmetic == SWE_ARITH_FAST) return fast_launch_adj_spatial(a, level_blocks, pred, s);
+    return launch_adj_spatial<ExactMath>(a, level_blocks, pred, s);
+}
+
+int adj_spatial(const float* S, const float* bed, int bedB, int B, int ny, int nx,
+                const swe_params* p, const float* level, int levelB, const float* lam_rhs,
+                float* scratch_cx, float* scratch_cy, float* lam_S, float* level_part,
+                int level_blocks, float* lam_bed, void* stream) {
+    AdjArgs a;
+    const int rc = adj_args(a, S, bed, bedB, B, ny, nx, p, level, levelB, lam_rhs, scratch_cx,
+                            scratch_cy, level_part, level_blocks, lam_bed);
+    if (rc != SWE_OK) return rc;
+    if (!lam_S) return SWE_EARG;
+    a.lS = lam_S;
+    return run_spatial(a, p, level_blocks, false, stream);
 }
 }  // namespace
 
@@ -603,6 +92,27 @@ extern "C" int swe_adj_spatial_bed_f32(const float* S, const float* bed, int bed
     if (!lam_bed) return SWE_EARG;
     return adj_spatial(S, bed, bedB, B, ny, nx, p, level, levelB, lam_rhs, scratch_cx, scratch_cy,
                        lam_S, level_part, level_blocks, lam_bed, stream);
+}
+
+extern "C" int swe_adj_stage2_f32(const float* P, const float* U, const float* k1, const float* bed,
+                                  int bedB, int B, int ny, int nx, const swe_params* p,
+                                  const float* level, int levelB, const float* lam_k2,
+                                  float* scratch_cx, float* scratch_cy, float dt,
+                                  const float* dt_dev, float* lam_U, float* lam_k1,
+                                  float* level_part, int level_blocks, float* lam_bed,
+                                  void* stream) {
+    AdjArgs a;
+    const int rc = adj_args(a, P, bed, bedB, B, ny, nx, p, level, levelB, lam_k2, scratch_cx,
+                            scratch_cy, level_part, level_blocks, lam_bed);
+    if (rc != SWE_OK) return rc;
+    if (!U || !k1 || !lam_U || !lam_k1) return SWE_EARG;
+    a.U = U;
+    a.k1 = k1;
+    a.dt = dt;
+    a.dt_dev = dt_dev;
+    a.lU = lam_U;
+    a.lk1 = lam_k1;
+    return run_spatial(a, p, level_blocks, true, stream);
 }
 
 namespace {
@@ -635,8 +145,9 @@ int adj_pointwise(int mode, const float* U, const float* k, const float* n, int 
     a.friction = p->apply_friction;
     a.friction_model = p->friction_model;
     a.kc = make_consts(*p);
-    adj_pointwise_kernel<<<blocks_for((long long)B * ny * nx), ADJ_THREADS, 0, (cudaStream_t)stream>>>(a);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (p->arithmetic == SWE_ARITH_FAST) return fast_launch_adj_pointwise(a, s);
+    return launch_adj_pointwise<ExactMath>(a, s);
 }
 }  // namespace
 

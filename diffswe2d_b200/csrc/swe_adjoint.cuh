@@ -15,6 +15,9 @@
 // bed's adjoint is not formed.
 #pragma once
 
+#include <math.h>
+
+#include "swe_approx.cuh"
 #include "swe_math.cuh"
 
 namespace swe {
@@ -72,14 +75,50 @@ SWE_HD void incr_bwd(const Incr& r, float lam, float theta, float& lqm, float& l
     lqp += lb + lc;
 }
 
+// Arithmetic of the adjoint's quotients, reciprocals and roots, a policy
+// class M of every function below:
+//   ExactMath: the correctly-rounded forms of the IEEE step (swe_math.cuh),
+//              for adjoints of runs made with SWE_ARITH_EXACT;
+//   FastMath:  the hardware approximations of the tolerance-mode step
+//              (swe_approx.cuh), for runs made with SWE_ARITH_FAST.
+// div(a, b, y) is a / b with y = rcp(b) shared by the quotients of one
+// denominator; pow(x, t) is x^t for positive normal x.
+struct ExactMath {
+    static SWE_HD float rcp(float b) { return shared_rcp(b); }
+    static SWE_HD float div(float a, float b, float y) { return quot(a, b, y); }
+    static SWE_HD float sqrt(float x) { return root(x); }
+    static SWE_HD float inv(float b) { return recip(b); }
+    static SWE_HD float pow(float x, float t) { return pow_pos(x, t); }
+    static SWE_HD float ln(float x) { return (float)::log((double)x); }
+};
+
+struct FastMath {
+#if defined(__CUDA_ARCH__)
+    static __device__ __forceinline__ float rcp(float b) { return rcpa(b); }
+    static __device__ __forceinline__ float div(float a, float, float y) { return a * y; }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrta(x); }
+    static __device__ __forceinline__ float inv(float b) { return rcpa(b); }
+    static __device__ __forceinline__ float pow(float x, float t) { return ex2a(t * lg2a(x)); }
+    static __device__ __forceinline__ float ln(float x) { return 0.69314718f * lg2a(x); }
+#else
+    static inline float rcp(float b) { return 1.0f / b; }
+    static inline float div(float a, float b, float) { return a / b; }
+    static inline float sqrt(float x) { return ::sqrtf(x); }
+    static inline float inv(float b) { return 1.0f / b; }
+    static inline float pow(float x, float t) { return ::powf(x, t); }
+    static inline float ln(float x) { return ::logf(x); }
+#endif
+};
+
 // Forward values of one cell kept for the backward pass.
 struct PrimRec {
     float U0, U1, U2, z;
     float h, safe, u, v, eta;
-    float rsafe;  // shared_rcp(safe): every quotient by safe uses it
+    float rsafe;  // M::rcp(safe): every quotient by safe uses it
     bool wet;
 };
 
+template <class M>
 SWE_HD PrimRec prim_rec(float U0, float U1, float U2, float z, const SweConsts& k) {
     PrimRec p;
     p.U0 = U0;
@@ -89,9 +128,9 @@ SWE_HD PrimRec prim_rec(float U0, float U1, float U2, float z, const SweConsts& 
     p.h = fmaxf(U0, 0.0f);
     p.wet = p.h > k.dry;
     p.safe = fmaxf(p.h, k.floor_h);
-    p.rsafe = shared_rcp(p.safe);
-    p.u = p.wet ? quot(U1, p.safe, p.rsafe) : 0.0f;
-    p.v = p.wet ? quot(U2, p.safe, p.rsafe) : 0.0f;
+    p.rsafe = M::rcp(p.safe);
+    p.u = p.wet ? M::div(U1, p.safe, p.rsafe) : 0.0f;
+    p.v = p.wet ? M::div(U2, p.safe, p.rsafe) : 0.0f;
     p.eta = p.h + z;
     return p;
 }
@@ -99,14 +138,15 @@ SWE_HD PrimRec prim_rec(float U0, float U1, float U2, float z, const SweConsts& 
 // Adjoint of primitive() + eta = h + bed (riemann.py:20-38,
 // reconstruction.py:23-24, :71-73): lh includes everything that reached h
 // (directly, via eta and via the reconstruction's own clamp of h).
+template <class M>
 SWE_HD void prim_bwd(const PrimRec& p, float lh, float lsafe, float lu, float lv, float leta,
                      const SweConsts& k, float& lU0, float& lU1, float& lU2, float& lz) {
     lh += leta;
     lz += leta;  // eta = h + bed
     if (p.wet) {
-        lU1 += quot(lu, p.safe, p.rsafe);
-        lU2 += quot(lv, p.safe, p.rsafe);
-        lsafe -= lu * quot(p.u, p.safe, p.rsafe) + lv * quot(p.v, p.safe, p.rsafe);
+        lU1 += M::div(lu, p.safe, p.rsafe);
+        lU2 += M::div(lv, p.safe, p.rsafe);
+        lsafe -= lu * M::div(p.u, p.safe, p.rsafe) + lv * M::div(p.v, p.safe, p.rsafe);
     }
     if (p.h >= k.floor_h) lh += lsafe;
     if (p.U0 >= 0.0f) lU0 += lh;
@@ -122,6 +162,7 @@ struct SideRec {
     Side s;
 };
 
+template <class M>
 SWE_HD SideRec side_fwd(const PrimRec& a, const PrimRec& c, const PrimRec& b, bool plus,
                         const SweConsts& k, bool wsr) {
     SideRec r;
@@ -141,7 +182,7 @@ SWE_HD SideRec side_fwd(const PrimRec& a, const PrimRec& c, const PrimRec& b, bo
         if (r.reset) deta = dh + dz;
     }
     const float hdh = 0.5f * dh;
-    r.q = quot(hdh, c.safe, c.rsafe);
+    r.q = M::div(hdh, c.safe, c.rsafe);
     if (plus) {
         r.s.hlin = c.h + hdh;
         r.s.eta = c.eta + 0.5f * deta;
@@ -170,7 +211,7 @@ struct PrimAdj {
     float h, safe, u, v, eta, z;
 };
 
-template <bool BEDG>
+template <bool BEDG, class M>
 SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin, float l_eta,
                      float l_u, float l_v, float l_bed, const SweConsts& k, PrimAdj& la,
                      PrimAdj& lc, PrimAdj& lb) {
@@ -187,8 +228,8 @@ SWE_HD void side_bwd(const SideRec& r, const PrimRec& c, bool plus, float l_hlin
     float l_fraw = (r.f_raw >= -10.0f && r.f_raw <= 10.0f) ? l_f : 0.0f;
     float l_q = c.h > k.dry ? -sg * l_fraw : 0.0f;
     // q = (0.5 dh) / safe
-    float l_dh = 0.5f * quot(l_q, c.safe, c.rsafe);
-    lc.safe -= l_q * quot(r.q, c.safe, c.rsafe);
+    float l_dh = 0.5f * M::div(l_q, c.safe, c.rsafe);
+    lc.safe -= l_q * M::div(r.q, c.safe, c.rsafe);
     // hlin = h +/- 0.5 dh ; eta_side = eta +/- 0.5 deta
     lc.h += l_hlin;
     l_dh += sg * (0.5f * l_hlin);
@@ -219,12 +260,12 @@ struct CellAdj {
     float U0, U1, U2, Z;  // Z: adjoint of the cell's bed (BEDG only)
 };
 
-template <bool BEDG>
+template <bool BEDG, class M>
 SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, float l_tan,
                      bool normal_y, const SweConsts& k, bool wsr, CellAdj out[4]) {
     // ---- forward: sides of p1 ("p") and p2 ("m")
-    const SideRec SL_ = side_fwd(P[0], P[1], P[2], true, k, wsr);
-    const SideRec SR_ = side_fwd(P[1], P[2], P[3], false, k, wsr);
+    const SideRec SL_ = side_fwd<M>(P[0], P[1], P[2], true, k, wsr);
+    const SideRec SR_ = side_fwd<M>(P[1], P[2], P[3], false, k, wsr);
     const Side& Lp = SL_.s;
     const Side& Rm = SR_.s;
     // face reconstruction (reconstruction.py:59-106)
@@ -241,10 +282,10 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     const float hL = fmaxf(hcL, 0.0f), hR = fmaxf(hcR, 0.0f);
     const bool wetL = hL > k.dry, wetR = hR > k.dry;
     const float safeL = fmaxf(hL, k.floor_h), safeR = fmaxf(hR, k.floor_h);
-    const float ysL = shared_rcp(safeL), ysR = shared_rcp(safeR);
-    const float uL = wetL ? quot(UL1, safeL, ysL) : 0.0f, vL = wetL ? quot(UL2, safeL, ysL) : 0.0f;
-    const float uR = wetR ? quot(UR1, safeR, ysR) : 0.0f, vR = wetR ? quot(UR2, safeR, ysR) : 0.0f;
-    const float cL = wetL ? root(k.g * safeL) : 0.0f, cR = wetR ? root(k.g * safeR) : 0.0f;
+    const float ysL = M::rcp(safeL), ysR = M::rcp(safeR);
+    const float uL = wetL ? M::div(UL1, safeL, ysL) : 0.0f, vL = wetL ? M::div(UL2, safeL, ysL) : 0.0f;
+    const float uR = wetR ? M::div(UR1, safeR, ysR) : 0.0f, vR = wetR ? M::div(UR2, safeR, ysR) : 0.0f;
+    const float cL = wetL ? M::sqrt(k.g * safeL) : 0.0f, cR = wetR ? M::sqrt(k.g * safeR) : 0.0f;
     const float unL = normal_y ? vL : uL, utL = normal_y ? uL : vL;
     const float unR = normal_y ? vR : uR, utR = normal_y ? uR : vR;
     const float us = (0.5f * (unL + unR) + cL) - cR;
@@ -263,8 +304,8 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     const float numh = (SR * fhL - SL * fhR) + SLSR * (hR - hL);
     const float mom = hR * unR - hL * unL;
     const float numq = (SR * fqL - SL * fqR) + SLSR * mom;
-    const float yden = shared_rcp(den);
-    const float fhs = quot(numh, den, yden), fqs = quot(numq, den, yden);
+    const float yden = M::rcp(den);
+    const float fhs = M::div(numh, den, yden), fqs = M::div(numq, den, yden);
     const bool lf = SL >= 0.0f, rf = SR <= 0.0f;
     const float fh = lf ? fhL : (rf ? fhR : fhs);
     const bool both = ldry && rdry;
@@ -294,8 +335,8 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
         l_fqs = l_fq;
     }
     // fhs = numh / den, fqs = numq / den
-    const float l_numh = quot(l_fhs, den, yden), l_numq = quot(l_fqs, den, yden);
-    const float l_den = -(l_fhs * quot(fhs, den, yden)) - l_fqs * quot(fqs, den, yden);
+    const float l_numh = M::div(l_fhs, den, yden), l_numq = M::div(l_fqs, den, yden);
+    const float l_den = -(l_fhs * M::div(fhs, den, yden)) - l_fqs * M::div(fqs, den, yden);
     float l_SL = 0.0f, l_SR = 0.0f, l_hL = 0.0f, l_hR = 0.0f, l_unL = 0.0f, l_unR = 0.0f;
     float l_cL = 0.0f, l_cR = 0.0f;
     // numh = (SR fhL - SL fhR) + SLSR (hR - hL)
@@ -376,18 +417,18 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     // primitive() of the face states
     float l_UL1 = 0.0f, l_UL2 = 0.0f, l_UR1 = 0.0f, l_UR2 = 0.0f, l_safeL = 0.0f, l_safeR = 0.0f;
     if (wetL) {
-        l_UL1 = quot(l_uL, safeL, ysL);
-        l_UL2 = quot(l_vL, safeL, ysL);
-        l_safeL -= l_uL * quot(uL, safeL, ysL) + l_vL * quot(vL, safeL, ysL);
+        l_UL1 = M::div(l_uL, safeL, ysL);
+        l_UL2 = M::div(l_vL, safeL, ysL);
+        l_safeL -= l_uL * M::div(uL, safeL, ysL) + l_vL * M::div(vL, safeL, ysL);
         const float c2 = 2.0f * cL;
-        l_safeL += k.g * quot(l_cL, c2, shared_rcp(c2));
+        l_safeL += k.g * M::div(l_cL, c2, M::rcp(c2));
     }
     if (wetR) {
-        l_UR1 = quot(l_uR, safeR, ysR);
-        l_UR2 = quot(l_vR, safeR, ysR);
-        l_safeR -= l_uR * quot(uR, safeR, ysR) + l_vR * quot(vR, safeR, ysR);
+        l_UR1 = M::div(l_uR, safeR, ysR);
+        l_UR2 = M::div(l_vR, safeR, ysR);
+        l_safeR -= l_uR * M::div(uR, safeR, ysR) + l_vR * M::div(vR, safeR, ysR);
         const float c2 = 2.0f * cR;
-        l_safeR += k.g * quot(l_cR, c2, shared_rcp(c2));
+        l_safeR += k.g * M::div(l_cR, c2, M::rcp(c2));
     }
     if (hL >= k.floor_h) l_hL += l_safeL;
     if (hR >= k.floor_h) l_hR += l_safeR;
@@ -440,12 +481,12 @@ SWE_HD void face_vjp(const PrimRec P[4], float l_mass, float l_nL, float l_nR, f
     l_Leta += l_inner * sa;
     l_Reta += l_inner * sb;
     // sides -> primitives of the four cells
-    side_bwd<BEDG>(SL_, P[1], true, l_Lhlin, l_Leta, l_Lu, l_Lv, l_Lbed, k, la[0], la[1], la[2]);
-    side_bwd<BEDG>(SR_, P[2], false, l_Rhlin, l_Reta, l_Ru, l_Rv, l_Rbed, k, la[1], la[2], la[3]);
+    side_bwd<BEDG, M>(SL_, P[1], true, l_Lhlin, l_Leta, l_Lu, l_Lv, l_Lbed, k, la[0], la[1], la[2]);
+    side_bwd<BEDG, M>(SR_, P[2], false, l_Rhlin, l_Reta, l_Ru, l_Rv, l_Rbed, k, la[1], la[2], la[3]);
     for (int i = 0; i < 4; ++i) {
         out[i].U0 = out[i].U1 = out[i].U2 = 0.0f;
         out[i].Z = la[i].z;  // sources, increments, face beds; prim_bwd adds the eta term
-        prim_bwd(P[i], la[i].h, la[i].safe, la[i].u, la[i].v, la[i].eta, k, out[i].U0, out[i].U1,
+        prim_bwd<M>(P[i], la[i].h, la[i].safe, la[i].u, la[i].v, la[i].eta, k, out[i].U0, out[i].U1,
                  out[i].U2, out[i].Z);
     }
 }

@@ -27,43 +27,12 @@
 // FP32-vs-FP64 difference of the FP64 reference, identical wet/dry masks.
 #include <cuda_runtime.h>
 
+#include "swe_approx.cuh"
 #include "swe_ensemble.cuh"
 #include "swe_sweep.cuh"
 
 namespace swe {
 namespace {
-
-__device__ __forceinline__ float rcpa(float x) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float sqrta(float x) {
-    float y;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float ex2a(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float lg2a(float x) {
-    float y;
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-// Three-input minimum / maximum (sm_100).
-__device__ __forceinline__ float min3f(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-__device__ __forceinline__ float max3f(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
 
 // Constants of the tolerance mode, derived from SweConsts in each thread.
 struct FK {

@@ -59,13 +59,12 @@ extern "C" {
  *   SWE_ARITH_FAST: the same step within FP32 rounding of the reference
  *     (fused multiply-adds, hardware reciprocal / square root / exp2 / log2
  *     approximations, algebraic identities of the reference's expressions);
- *     about three times the throughput.  After 1000 steps of the 256x256
- *     island case every field stays within 1.5x the reference's own
- *     FP32-vs-FP64 difference of the FP64 reference, with identical wet/dry
- *     masks.
+ *     about twice the throughput.  After 1000 steps of the 256x256 island
+ *     case every field stays within 1.5x the reference's own FP32-vs-FP64
+ *     difference of the FP64 reference, with identical wet/dry masks.
  * The mode selects the kernels of swe_spatial_operator_f32, the swe_step_*
- * entry points and the ensemble; the operator-level entry points and the
- * adjoint are always IEEE. */
+ * entry points, the ensemble and the step adjoint (swe_adj_*); the
+ * operator-level entry points are always IEEE. */
 #define SWE_ARITH_EXACT 0
 #define SWE_ARITH_FAST 1
 
@@ -288,7 +287,10 @@ int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB, 
 
 /* ---------------------------------------------------------------------
  * Adjoint of the step (the reference's autograd gradient through
- * SWE2D.step, src/solver.py:572-663, with dt detached as in :626).
+ * SWE2D.step, src/solver.py:572-663, with dt detached as in :626).  The
+ * arithmetic follows p->arithmetic: SWE_ARITH_EXACT evaluates the adjoint
+ * with correctly-rounded quotients and roots, SWE_ARITH_FAST with the
+ * hardware approximations of the tolerance-mode step.
  * --------------------------------------------------------------------- */
 
 /*
@@ -319,6 +321,26 @@ int swe_adj_spatial_bed_f32(const float* S, const float* bed, int bedB, int B, i
                             const float* lam_rhs, float* scratch_cx, float* scratch_cy,
                             float* lam_S, float* level_part, int level_blocks, float* lam_bed,
                             void* stream);
+
+/*
+ * Stage 2's spatial adjoint and predictor adjoint together: with
+ * P = clean(U, U + dt/2 k1) the step's predictor (solver.py:639) and lam_k2
+ * the adjoint of k2 = rhs(P), lam_U += (dP/dU)^T lam_P and
+ * lam_k1 = (dP/dk1)^T lam_P (written), where lam_P = (d rhs / d P)^T lam_k2
+ * is formed per cell and not stored.  The same result as
+ * swe_adj_spatial_f32(P, ..., lam_S = a zeroed lam_P) followed by
+ * swe_adj_pointwise_f32(mode 1, U, k1, ..., lam_out = lam_P), in two
+ * launches instead of three.  dt_dev, if not null, holds the step's dt in
+ * device memory (read in place of dt, for captured graphs).  lam_bed may be
+ * null; if not, the bed's adjoint is accumulated as in
+ * swe_adj_spatial_bed_f32 (with its 16-float scratch records).  lam_k1 may
+ * be the lam_k2 buffer itself (it is written after the last read of lam_k2).
+ */
+int swe_adj_stage2_f32(const float* P, const float* U, const float* k1, const float* bed, int bedB,
+                       int B, int ny, int nx, const swe_params* p, const float* level, int levelB,
+                       const float* lam_k2, float* scratch_cx, float* scratch_cy, float dt,
+                       const float* dt_dev, float* lam_U, float* lam_k1, float* level_part,
+                       int level_blocks, float* lam_bed, void* stream);
 
 /*
  * Pointwise parts of the step adjoint, for step input U, tendency k and

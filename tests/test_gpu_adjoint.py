@@ -79,6 +79,105 @@ def test_one_step_vjp_matches_reference_autograd(golden, case):
         assert _rel(gn, d[f"{case}_gn"]) <= TOL
 
 
+@pytest.mark.parametrize("case", sorted(STEP_CASES))
+def test_one_step_vjp_fast_arithmetic(golden, case):
+    """The tolerance-mode adjoint (hardware reciprocal / square root, FMA
+    contraction) at the tolerance-mode step: within 1e-4 of the reference's
+    FP32 autograd, or, where the reference's own FP32 and FP64 gradients
+    differ by more, within 1.5x that difference of the FP64 gradient."""
+    d = golden("adj_step")
+    kw = STEP_CASES[case]
+    field = d["z0"] if kw.get("frictionmodel") == "roughness_length" else d["n"]
+    cfg = SWEConfig(**kw, constant_value=0.05)
+    m = SWE2D(_t(d["bed"]), _t(field), 0.05, 0.04, config=cfg, train_dem=False, arithmetic="fast")
+    m.roughness_length.requires_grad_(True)
+    U = _t(d["U"]).requires_grad_(True)
+    lv = torch.tensor(0.18, device=DEV, requires_grad=True)
+    Un, dt = m.step(U, 0.0, 0.01, boundary_level=lv)
+    assert dt == pytest.approx(float(d[f"{case}_dt"]), rel=1e-5)
+    (Un * _t(d["w"])).sum().backward()
+    gU = U.grad.cpu().numpy()
+    eU, eU64 = _rel(gU, d[f"{case}_gU"]), _rel(gU, d[f"{case}_gU64"])
+    floor = _rel(d[f"{case}_gU"], d[f"{case}_gU64"])
+    print(case, "fast dL/dU vs FP32 autograd", eU, "vs FP64", eU64, "FP32-vs-FP64", floor)
+    assert eU <= TOL or eU64 <= 1.5 * floor
+    gl, rl = float(lv.grad), float(d[f"{case}_glevel"])
+    if rl != 0.0:
+        assert abs(gl - rl) <= TOL * abs(rl)
+    else:
+        assert gl == 0.0
+    if kw.get("apply_friction", True):
+        assert _rel(m.roughness_length.grad.cpu().numpy(), d[f"{case}_gn"]) <= TOL
+
+
+@pytest.mark.parametrize("arithmetic", ["exact", "fast"])
+@pytest.mark.parametrize("bed_grad", [False, True])
+def test_stage2_entry_equals_spatial_then_predictor(golden, arithmetic, bed_grad):
+    """swe_adj_stage2_f32 (spatial adjoint at P with the predictor adjoint
+    fused into its gather) against swe_adj_spatial(_bed)_f32 into a zeroed
+    lam_P followed by swe_adj_pointwise_f32 mode 1: the same adjoints of U,
+    k1, the level and the bed -- bit for bit in the IEEE mode, within 1e-6
+    (normwise) in the tolerance mode."""
+    from diffswe2d_b200 import _native as nat
+    from diffswe2d_b200.adjoint import LEVEL_BLOCKS
+    d = golden("adj_step")
+    cfg = SWEConfig(**STEP_CASES["mixed_a"], constant_value=0.05)
+    m = SWE2D(_t(d["bed"]), _t(d["n"]), 0.05, 0.04, config=cfg, train_dem=False,
+              arithmetic=arithmetic)
+    lib, st, p = nat.lib(), nat.stream_handle(torch.device(DEV)), m._params()
+    U = _t(d["U"])
+    B, _, ny, nx = U.shape
+    bed = m.bed.detach().reshape(1, 1, ny, nx).contiguous()
+    lv = torch.tensor([0.18], device=DEV)
+    red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=DEV)
+    K1, P = torch.empty_like(U), torch.empty_like(U)
+    nat.check(lib.swe_spatial_operator_f32(nat.ptr(U), nat.ptr(bed), B, 1, ny, nx, p, nat.ptr(lv), 1,
+                                           None, nat.FORCING_NONE, 1, None, nat.FORCING_NONE, 1,
+                                           nat.ptr(K1), nat.ptr(red), st), "k1")
+    dt = 2.5e-3
+    nat.check(lib.swe_adj_pointwise_f32(2, nat.ptr(U), nat.ptr(K1), None, 1, B, ny, nx, p, dt, None,
+                                        None, None, None, nat.ptr(P), st), "predictor")
+    g = torch.Generator(device="cpu").manual_seed(3)
+    lk2 = torch.randn(U.shape, generator=g).to(DEV)
+    base = torch.randn(U.shape, generator=g).to(DEV)
+    rec = 16 if bed_grad else 12
+    cx = torch.empty(B * ny * (nx + 1) * rec, device=DEV)
+    cy = torch.empty(B * (ny + 1) * nx * rec, device=DEV)
+
+    def run(fused):
+        lamU, lk1 = base.clone(), torch.zeros_like(U)
+        part = torch.zeros(B * LEVEL_BLOCKS, device=DEV)
+        lbed = torch.zeros((B, ny, nx), device=DEV) if bed_grad else None
+        if fused:
+            rc = lib.swe_adj_stage2_f32(nat.ptr(P), nat.ptr(U), nat.ptr(K1), nat.ptr(bed), 1, B, ny, nx,
+                                        p, nat.ptr(lv), 1, nat.ptr(lk2), nat.ptr(cx), nat.ptr(cy), dt,
+                                        None, nat.ptr(lamU), nat.ptr(lk1), nat.ptr(part), LEVEL_BLOCKS,
+                                        nat.ptr(lbed) if bed_grad else None, st)
+            nat.check(rc, "stage 2")
+        else:
+            lamP = torch.zeros_like(U)
+            args = (nat.ptr(P), nat.ptr(bed), 1, B, ny, nx, p, nat.ptr(lv), 1, nat.ptr(lk2), nat.ptr(cx),
+                    nat.ptr(cy), nat.ptr(lamP), nat.ptr(part), LEVEL_BLOCKS)
+            if bed_grad:
+                nat.check(lib.swe_adj_spatial_bed_f32(*args, nat.ptr(lbed), st), "spatial")
+            else:
+                nat.check(lib.swe_adj_spatial_f32(*args, st), "spatial")
+            nat.check(lib.swe_adj_pointwise_f32(1, nat.ptr(U), nat.ptr(K1), None, 1, B, ny, nx, p, dt,
+                                                nat.ptr(lamP), nat.ptr(lamU), nat.ptr(lk1), None, None,
+                                                st), "predictor adjoint")
+        torch.cuda.synchronize()
+        out = [lamU, lk1, part] + ([lbed] if bed_grad else [])
+        return [x.cpu().numpy() for x in out]
+
+    fused, split = run(True), run(False)
+    assert np.abs(split[1]).max() > 0 and np.abs(split[2]).max() > 0
+    for a, b in zip(fused, split):
+        if arithmetic == "exact":
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        else:
+            assert _rel(a, b) <= 1e-6
+
+
 def _run_model(d, requires=True, arithmetic="exact"):
     cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
                     boundary_bottom="wall")
