@@ -39,6 +39,12 @@ from .adjoint import LEVEL_BLOCKS, AdjointStepper, bed_input
 
 GRAPH_STEPS = 32
 CHECKPOINT_EVERY = 128
+# Kernels of this library per solver step: forward (stage 1, stage 2, the
+# run clock) and adjoint with the stage-1 tendency kept (cursor set-up,
+# predictor, k2 tendency, corrector adjoint, stage-2 spatial + predictor
+# adjoint (2), stage-1 spatial adjoint (2), cursor finish).
+FORWARD_KERNELS_PER_STEP = 3
+ADJOINT_KERNELS_PER_STEP = 9
 
 
 class GaugeRunWorkspace:
@@ -86,6 +92,7 @@ class GaugeRunWorkspace:
         self.replay_graph = None
         self.last_steps = 0
         self.generation = 0
+        self.kernel_launches = 0  # kernels of this library enqueued or replayed so far
         self.stepper = None
         # full-trajectory storage (None: when free device memory allows)
         self.store_mode = store_states
@@ -152,6 +159,7 @@ class GaugeRunWorkspace:
         self.gauge_out.zero_()
         self._set_clock()
         self._tick(self.bufs[0])
+        self.kernel_launches += 1
         if self.fwd_graph is None:
             from .autotune import sweep_rows
             nat.load_kernels()
@@ -181,6 +189,7 @@ class GaugeRunWorkspace:
                     self.ckpts.append(torch.empty_like(self.bufs[0]))
                 self.ckpts[j].copy_(self.bufs[0])
             (self.fwd_store_graph if storing else self.fwd_graph).replay()
+            self.kernel_launches += self.G * FORWARD_KERNELS_PER_STEP
             if storing:
                 storing = self._keep_replay(replay)
             replay += 1
@@ -247,6 +256,7 @@ class GaugeRunWorkspace:
         self.seg[0].copy_(self.ckpts[j])
         self._set_clock(replay=1, replay_end=s1, steps=s0, active=0)
         self._tick(self.seg[0])
+        self.kernel_launches += 1 + self.k * FORWARD_KERNELS_PER_STEP
         if self.replay_graph is None:
             from .autotune import sweep_rows
             g = torch.cuda.CUDAGraph()
@@ -330,6 +340,7 @@ class GaugeRunWorkspace:
                 self._recompute_segment(j, s0, s1)
             self.cursor.fill_(s1 - 1)
             count = s1 - s0
+            self.kernel_launches += count * ADJOINT_KERNELS_PER_STEP
             if count < self.k:
                 self._adjoint_steps(count)
                 if count % 2:
