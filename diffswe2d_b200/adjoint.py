@@ -26,7 +26,11 @@ import torch
 
 from . import _native as nat
 
-LEVEL_BLOCKS = 64
+def level_blocks(ny: int, nx: int) -> int:
+    """Blocks per batch member of the spatial adjoint's gather launch (one
+    cell per thread of 256, at most 1024 blocks): each writes one partial
+    sum of the level adjoint, summed in a fixed order afterwards."""
+    return max(1, min(1024, -(-ny * nx // 256)))
 
 
 def bed_input(model):
@@ -55,7 +59,8 @@ class AdjointStepper:
         self.cy = torch.empty(B * (ny + 1) * nx * rec, device=dev)
         # bed adjoint per batch member, accumulated over the steps of a pass
         self.lam_bed = torch.zeros((B, ny, nx), device=dev) if self.bed_grad else None
-        self.part = torch.empty((2, B * LEVEL_BLOCKS), device=dev)
+        self.level_blocks = level_blocks(ny, nx)
+        self.part = torch.empty((2, B * self.level_blocks), device=dev)
         probe = torch.empty((B, 1, ny, nx), device=dev)
         self.bed, self.n = model._fields(probe.expand(B, 3, ny, nx))
         self.infil, self.imode, self.iB = model._forcing_arg(infiltration, probe)
@@ -80,7 +85,7 @@ class AdjointStepper:
     def _spatial(self, S, lv, lam_rhs, lam_S, part, what):
         args = (nat.ptr(S), nat.ptr(self.bed), self.bed.shape[0], self.B, self.ny, self.nx, self.p,
                 nat.ptr(lv), self.levelB, nat.ptr(lam_rhs), nat.ptr(self.cx), nat.ptr(self.cy),
-                nat.ptr(lam_S), nat.ptr(part), LEVEL_BLOCKS)
+                nat.ptr(lam_S), nat.ptr(part), self.level_blocks)
         if self.bed_grad:
             rc = self.lib.swe_adj_spatial_bed_f32(*args, nat.ptr(self.lam_bed), self.st)
         else:
@@ -96,7 +101,7 @@ class AdjointStepper:
             nat.ptr(P), nat.ptr(U), nat.ptr(K1), nat.ptr(self.bed), self.bed.shape[0], self.B, self.ny,
             self.nx, self.p, nat.ptr(lv), self.levelB, nat.ptr(self.lam_k), nat.ptr(self.cx),
             nat.ptr(self.cy), 0.0 if dev_dt else float(dt), nat.ptr(dt) if dev_dt else None,
-            nat.ptr(lam_U), nat.ptr(self.lam_k), nat.ptr(self.part[0]), LEVEL_BLOCKS,
+            nat.ptr(lam_U), nat.ptr(self.lam_k), nat.ptr(self.part[0]), self.level_blocks,
             nat.ptr(self.lam_bed) if self.bed_grad else None, self.st)
         nat.check(rc, "adjoint spatial operator and predictor (stage 2)")
 
@@ -129,7 +134,7 @@ class AdjointStepper:
         adjoint (when friction is on) for the step at input state U with
         level vector lv and time step dt (a float, or a one-element device
         tensor); returns the level adjoint's partial sums
-        [2, B * LEVEL_BLOCKS] (their sum per batch member is that member's
+        [2, B * level_blocks] (their sum per batch member is that member's
         level adjoint).  K1, if given, is the step's stage-1 tendency kept
         from the forward recompute (else it is recomputed here)."""
         K2, P, lam_k = self.K2, self.P, self.lam_k
@@ -149,7 +154,7 @@ class AdjointStepper:
 
     def level_adjoint(self, part):
         """Level adjoint [levelB] from the partial sums of one step."""
-        lam = part.view(2, self.B, LEVEL_BLOCKS).sum(dim=(0, 2))
+        lam = part.view(2, self.B, self.level_blocks).sum(dim=(0, 2))
         return lam.sum(0, keepdim=True) if self.levelB == 1 else lam
 
 

@@ -23,17 +23,25 @@
 namespace swe {
 
 constexpr int ADJ_THREADS = 256;
-// The face and gather kernels are latency-bound at low occupancy; three
-// blocks per SM (a few hundred bytes of spills in the face kernel) measured
-// 2.5-9 % faster per inversion iteration than two.
+// Blocks per SM the kernels are compiled for (register budgets): the face
+// kernel at three (80 registers, a few hundred bytes of spills) measured
+// 2.5-9 % faster per inversion iteration than at two (no spills) and 3 %
+// faster than at four; the gather kernel is memory-latency bound and runs
+// 7 % faster per adjoint step at eight (32 registers) than at three.
+#ifndef SWE_ADJ_FACE_MINB
+#define SWE_ADJ_FACE_MINB 3
+#endif
+#ifndef SWE_ADJ_GATHER_MINB
+#define SWE_ADJ_GATHER_MINB 8
+#endif
 
 struct AdjArgs {
     const float* S;      // state whose tendency is differentiated, [B,3,ny,nx]
     const float* bed;    // [bedB,1,ny,nx]
     const float* level;  // [levelB]
     const float* lrhs;   // adjoint of the tendency, [B,3,ny,nx]
-    float* cx;           // x-face contributions [B][ny][nx+1][12]
-    float* cy;           // y-face contributions [B][ny+1][nx][12]
+    float* cx;           // x-face contributions [12 or 16 planes][B][ny][nx+1]
+    float* cy;           // y-face contributions [12 or 16 planes][B][ny+1][nx]
     float* lS;           // adjoint of S, accumulated (+=)
     float* llevel_part;  // per-block partial level adjoints [B][gridDim.x]
     float* lbed;         // adjoint of the bed [B,ny,nx], accumulated (+=); BEDG only
@@ -71,9 +79,6 @@ struct PwArgs {
 };
 
 namespace {
-
-
-
 
 __device__ __forceinline__ size_t a3(int b, int c, int j, int i, int ny, int nx) {
     return (((size_t)b * 3 + c) * ny + j) * nx + i;
@@ -127,9 +132,15 @@ __device__ PrimRec padded_prim(const AdjArgs& a, int b, int j, int i) {
     return prim_rec<M>(U0, U1, U2, z, a.kc);
 }
 
-// Face records: 4 cells x (U0, U1, U2[, Z]) floats.
+// Face records: 4 cells x (U0, U1, U2[, Z]) floats per face, stored as
+// planes (plane p = cell * C + channel, C = 3 or 4; within a plane, face t of
+// the launch at t) so that consecutive faces' writes and consecutive cells'
+// reads are coalesced.
 template <bool BEDG>
 __host__ __device__ constexpr int rec_floats() { return BEDG ? 16 : 12; }
+
+__device__ __forceinline__ size_t xfaces(const AdjArgs& a) { return (size_t)a.B * a.ny * (a.nx + 1); }
+__device__ __forceinline__ size_t yfaces(const AdjArgs& a) { return (size_t)a.B * (a.ny + 1) * a.nx; }
 
 // Faces of one direction, one thread per face, over blocks [blk, blk + nblk)
 // of the launch.
@@ -152,7 +163,19 @@ __device__ __forceinline__ void face_dir(const AdjArgs& a, int blk, int nblk) {
             f = (int)(r - (long long)row * (nx + 1));
         }
         PrimRec P[4];
-        for (int s = 0; s < 4; ++s) P[s] = DIRY ? padded_prim<M>(a, b, f - 2 + s, row) : padded_prim<M>(a, b, row, f - 2 + s);
+        if (f >= 2 && f <= (DIRY ? ny : nx) - 2) {  // the stencil's four cells are interior
+            const size_t o0 = DIRY ? a3(b, 0, f - 2, row, ny, nx) : a3(b, 0, row, f - 2, ny, nx);
+            const size_t z0 = DIRY ? ((size_t)(a.bedB == 1 ? 0 : b) * ny + (f - 2)) * nx + row
+                                   : ((size_t)(a.bedB == 1 ? 0 : b) * ny + row) * nx + (f - 2);
+            const size_t step = DIRY ? (size_t)nx : 1;
+            for (int s = 0; s < 4; ++s) {
+                const size_t o = o0 + s * step;
+                P[s] = prim_rec<M>(a.S[o], a.S[o + plane], a.S[o + 2 * plane], a.bed[z0 + s * step], a.kc);
+            }
+        } else {
+            for (int s = 0; s < 4; ++s)
+                P[s] = DIRY ? padded_prim<M>(a, b, f - 2 + s, row) : padded_prim<M>(a, b, row, f - 2 + s);
+        }
         // adjoints of the face outputs from the tendencies of the two cells
         // sharing the face: (F_right(f) - F_left(f+1)) / d
         const float d = DIRY ? a.kc.dy : a.kc.dx;
@@ -179,19 +202,20 @@ __device__ __forceinline__ void face_dir(const AdjArgs& a, int blk, int nblk) {
         CellAdj out[4];
         face_vjp<BEDG, M>(P, l_mass, l_nL, l_nR, l_tan, DIRY, a.kc, a.wsr != 0, out);
         constexpr int C = BEDG ? 4 : 3;
-        float* dst = (DIRY ? a.cy : a.cx) + (size_t)t * rec_floats<BEDG>();
+        const size_t np = DIRY ? yfaces(a) : xfaces(a);
+        float* dst = (DIRY ? a.cy : a.cx) + t;
         for (int s = 0; s < 4; ++s) {
-            dst[C * s] = out[s].U0;
-            dst[C * s + 1] = out[s].U1;
-            dst[C * s + 2] = out[s].U2;
-            if (BEDG) dst[C * s + 3] = out[s].Z;
+            dst[(C * s) * np] = out[s].U0;
+            dst[(C * s + 1) * np] = out[s].U1;
+            dst[(C * s + 2) * np] = out[s].U2;
+            if (BEDG) dst[(C * s + 3) * np] = out[s].Z;
         }
     }
 }
 
 // The x faces on the first xblocks blocks, the y faces on the rest.
 template <bool BEDG, class M>
-__global__ void __launch_bounds__(ADJ_THREADS, 3) adj_face_kernel(const AdjArgs a, int xblocks) {
+__global__ void __launch_bounds__(ADJ_THREADS, SWE_ADJ_FACE_MINB) adj_face_kernel(const AdjArgs a, int xblocks) {
     if ((int)blockIdx.x < xblocks) face_dir<false, BEDG, M>(a, blockIdx.x, xblocks);
     else face_dir<true, BEDG, M>(a, blockIdx.x - xblocks, gridDim.x - xblocks);
 }
@@ -200,29 +224,31 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) adj_face_kernel(const AdjArgs 
 // (l[3], the bed channel, with BEDG only).
 template <bool BEDG>
 __device__ void lam_x(const AdjArgs& a, int b, int j, int col, float l[4]) {
-    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
+    constexpr int C = BEDG ? 4 : 3;
+    const size_t np = xfaces(a);
     l[0] = l[1] = l[2] = l[3] = 0.0f;
     for (int f = col - 1; f <= col + 2; ++f) {
         if (f < 0 || f > a.nx) continue;
-        const float* c = a.cx + ((((size_t)b * a.ny + j) * (a.nx + 1) + f) * R) + C * (col - f + 2);
+        const float* c = a.cx + (((size_t)b * a.ny + j) * (a.nx + 1) + f) + C * (col - f + 2) * np;
         l[0] += c[0];
-        l[1] += c[1];
-        l[2] += c[2];
-        if (BEDG) l[3] += c[3];
+        l[1] += c[np];
+        l[2] += c[2 * np];
+        if (BEDG) l[3] += c[3 * np];
     }
 }
 
 template <bool BEDG>
 __device__ void lam_y(const AdjArgs& a, int b, int row, int i, float l[4]) {
-    constexpr int C = BEDG ? 4 : 3, R = rec_floats<BEDG>();
+    constexpr int C = BEDG ? 4 : 3;
+    const size_t np = yfaces(a);
     l[0] = l[1] = l[2] = l[3] = 0.0f;
     for (int f = row - 1; f <= row + 2; ++f) {
         if (f < 0 || f > a.ny) continue;
-        const float* c = a.cy + ((((size_t)b * (a.ny + 1) + f) * a.nx + i) * R) + C * (row - f + 2);
+        const float* c = a.cy + (((size_t)b * (a.ny + 1) + f) * a.nx + i) + C * (row - f + 2) * np;
         l[0] += c[0];
-        l[1] += c[1];
-        l[2] += c[2];
-        if (BEDG) l[3] += c[3];
+        l[1] += c[np];
+        l[2] += c[2 * np];
+        if (BEDG) l[3] += c[3 * np];
     }
 }
 
@@ -477,7 +503,7 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
 }
 
 template <bool BEDG, bool PRED, class M>
-__global__ void __launch_bounds__(ADJ_THREADS, 3) adj_gather_kernel(const AdjArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, SWE_ADJ_GATHER_MINB) adj_gather_kernel(const AdjArgs a) {
     const int ny = a.ny, nx = a.nx;
     const int b = blockIdx.y;
     const long long ncell = (long long)ny * nx;

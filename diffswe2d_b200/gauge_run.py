@@ -35,7 +35,7 @@ from typing import Optional, Sequence, Tuple
 import torch
 
 from . import _native as nat
-from .adjoint import LEVEL_BLOCKS, AdjointStepper, bed_input
+from .adjoint import AdjointStepper, bed_input
 
 GRAPH_STEPS = 32
 CHECKPOINT_EVERY = 128
@@ -297,7 +297,7 @@ class GaugeRunWorkspace:
                        K1=self.seg_k1[i])
             rc = lib.swe_gauge_adjoint_post_f32(
                 nat.ptr(self.cursor), nat.ptr(self.step_code), nat.ptr(part), 2, self.B,
-                LEVEL_BLOCKS, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)
+                stp.level_blocks, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)
             nat.check(rc, "gauge-run adjoint finish")
 
     def backward(self, g_gauges, g_final, bed_grad: bool = False):

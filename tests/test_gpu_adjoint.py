@@ -119,7 +119,7 @@ def test_stage2_entry_equals_spatial_then_predictor(golden, arithmetic, bed_grad
     k1, the level and the bed -- bit for bit in the IEEE mode, within 1e-6
     (normwise) in the tolerance mode."""
     from diffswe2d_b200 import _native as nat
-    from diffswe2d_b200.adjoint import LEVEL_BLOCKS
+    from diffswe2d_b200.adjoint import level_blocks
     d = golden("adj_step")
     cfg = SWEConfig(**STEP_CASES["mixed_a"], constant_value=0.05)
     m = SWE2D(_t(d["bed"]), _t(d["n"]), 0.05, 0.04, config=cfg, train_dem=False,
@@ -141,6 +141,7 @@ def test_stage2_entry_equals_spatial_then_predictor(golden, arithmetic, bed_grad
     lk2 = torch.randn(U.shape, generator=g).to(DEV)
     base = torch.randn(U.shape, generator=g).to(DEV)
     rec = 16 if bed_grad else 12
+    LEVEL_BLOCKS = level_blocks(ny, nx)
     cx = torch.empty(B * ny * (nx + 1) * rec, device=DEV)
     cy = torch.empty(B * (ny + 1) * nx * rec, device=DEV)
 
