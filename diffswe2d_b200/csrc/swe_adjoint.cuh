@@ -24,15 +24,8 @@ namespace swe {
 
 // Gradient shares of torch.minimum(a, b) (or maximum with larger = true).
 SWE_HD void minmax_shares(float a, float b, bool larger, float& sa, float& sb) {
-    if (a == b) {
-        sa = sb = 0.5f;
-    } else if ((a < b) != larger) {
-        sa = 1.0f;
-        sb = 0.0f;
-    } else {
-        sa = 0.0f;
-        sb = 1.0f;
-    }
+    sa = a == b ? 0.5f : (((a < b) != larger) ? 1.0f : 0.0f);
+    sb = 1.0f - sa;
 }
 
 // limited_increment of the middle of three values with the shares of each
@@ -48,20 +41,19 @@ SWE_HD Incr incr_fwd(float qm, float q, float qp, float theta) {
     const float c = theta * (qp - q);
     Incr r;
     r.val = minmod3(a, b, c);
-    const float sgn_a = (a > 0.0f) - (a < 0.0f), sgn_b = (b > 0.0f) - (b < 0.0f),
-                sgn_c = (c > 0.0f) - (c < 0.0f);
-    const bool same = (sgn_a == sgn_b) && (sgn_b == sgn_c) && sgn_a != 0.0f;
-    r.sa = r.sb = r.sc = 0.0f;
-    if (same) {
-        const float aa = fabsf(a), ab = fabsf(b), ac = fabsf(c);
-        const float inner = fminf(ab, ac);
-        float s_a, s_in, s_b, s_c;
-        minmax_shares(aa, inner, false, s_a, s_in);
-        minmax_shares(ab, ac, false, s_b, s_c);
-        r.sa = s_a;
-        r.sb = s_in * s_b;
-        r.sc = s_in * s_c;
-    }
+    // minmod3 passes gradient only when all three share a sign (a NaN
+    // compares false: no gradient), to the smallest of |a|, min(|b|, |c|)
+    // with torch.minimum's tie rule (half each on a tie): the shares of
+    // minmax_shares, written branch-free (s_in = 1 - s_a, s_c = 1 - s_b).
+    const bool same = (a > 0.0f && b > 0.0f && c > 0.0f) || (a < 0.0f && b < 0.0f && c < 0.0f);
+    const float aa = fabsf(a), ab = fabsf(b), ac = fabsf(c);
+    const float inner = fminf(ab, ac);
+    const float s_a = aa == inner ? 0.5f : (aa < inner ? 1.0f : 0.0f);
+    const float s_b = ab == ac ? 0.5f : (ab < ac ? 1.0f : 0.0f);
+    const float s_in = same ? 1.0f - s_a : 0.0f;
+    r.sa = same ? s_a : 0.0f;
+    r.sb = s_in * s_b;
+    r.sc = s_in * (1.0f - s_b);
     return r;
 }
 
