@@ -83,7 +83,8 @@ def parse():
     ap.add_argument("--reference-context", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--rows", type=int, default=0,
                     help="sweep tile height to use instead of the autotuner's (0: autotune)")
-    ap.add_argument("--workload", choices=["runup4096", "ensemble", "inversion", "warmstart"],
+    ap.add_argument("--workload", choices=["runup4096", "ensemble", "inversion", "warmstart",
+                                           "adjoint"],
                     default="runup4096",
                     help="runup4096: the headline single-grid step; ensemble: 64 scenarios of "
                          "uneven sizes in one persistent launch vs 64 sequential runs")
@@ -725,6 +726,69 @@ def run_inversion(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, world, rank, local):
+    """The step adjoint alone at the inversion's shape (--inv-cases runup
+    cases of --inv-grid, --inv-arithmetic): time per adjoint step as the
+    gauge run's backward pass runs it (predictor and k2 re-evaluated, k1
+    kept; corrector, stage-2 and stage-1 spatial adjoints), on a state after
+    0.3 s of inflow.  The timed loop is bracketed by cudaProfilerStart/Stop
+    (for `ncu --profile-from-start off`).  A step of the metric is one
+    adjoint step."""
+    from diffswe2d_b200.adjoint import AdjointStepper
+    from diffswe2d_b200.autotune import sweep_rows, tuned_rows_for_shape
+    from diffswe2d_b200.inversion import make_runup_problem
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    gy, gx, gdx = args.inv_grid.split("x")
+    gy, gx, gdx = int(gy), int(gx), float(gdx)
+    problem, _ = make_runup_problem(cases=args.inv_cases, seed=0, ny=gy, nx=gx, dx=gdx, duration=1.0,
+                                    dt_out=0.02, device=dev, arithmetic=args.inv_arithmetic)
+    m = problem.model
+    B = args.inv_cases
+    with torch.no_grad():
+        U, _ = m(problem.U0.clone(), t_end=0.3, boundary_level=torch.tensor(0.02, device=dev))
+    stp = AdjointStepper(m, B, gy, gx, dev, 1)
+    lv = torch.tensor([0.01], device=dev)
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    lam_out = (torch.randn(U.shape, generator=gen) * 1e-3).to(dev)
+    lam_U = torch.zeros_like(U)
+    lam_n = torch.zeros_like(stp.n)
+    dt = torch.tensor([1e-3], device=dev)
+    K1 = torch.empty_like(U)
+    rows = tuned_rows_for_shape(B, gy, gx, dev, arithmetic=args.inv_arithmetic)
+    clk = Clocks(local)
+    with sweep_rows(rows):
+        stp._tendency(U, lv, K1)
+        for _ in range(max(args.warmup, 1)):
+            stp(U, lv, dt, lam_out, lam_U, lam_n, K1=K1)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.profiler.start()
+        with clk:
+            e0.record()
+            for _ in range(args.steps):
+                stp(U, lv, dt, lam_out, lam_U, lam_n, K1=K1)
+            e1.record()
+            torch.cuda.synchronize(dev)
+        torch.cuda.profiler.stop()
+    us = e0.elapsed_time(e1) / args.steps * 1e3
+    line = {
+        "metric": "step adjoint time (inversion shape)", "value": us, "unit": "us",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": us / 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"runup_adjoint_{gy}x{gx}", "cases": B, "dx": gdx, "tile_rows": rows,
+                   "arithmetic": args.inv_arithmetic,
+                   "per_step": "predictor + k2 re-evaluation, corrector adjoint, stage-2 spatial + "
+                               "predictor adjoint, stage-1 spatial adjoint (k1 kept)"},
+        "adjoint_mcell_per_s": B * gy * gx / us,
+        "gradient_finite": bool(torch.isfinite(lam_U).all()),
+        "gpu_launches": 7 * args.steps, "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_warmstart(args, world, rank, local):
     """Config 5: learned warm start + adjoint inversion against the plain
     (cold-start) inversion, Adam lr 0.002, tolerance gauge RMSE <= 1e-4 m, on
@@ -812,9 +876,9 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    if args.workload == "inversion" and args.impl == "b200":
+    if args.workload in ("inversion", "adjoint") and args.impl == "b200":
         if rank == 0:
-            run_inversion(args, world, rank, local)
+            (run_inversion if args.workload == "inversion" else run_adjoint)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
