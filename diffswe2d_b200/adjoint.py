@@ -115,8 +115,9 @@ class AdjointStepper:
 
     def _pointwise(self, mode, U, k, dt, lam_out, lam_U, lam_n, P_out):
         n = self.n
-        nptr = nat.ptr(n) if mode == 0 else None
-        lnptr = nat.ptr(lam_n) if (mode == 0 and self.fric) else None
+        corrector = mode in (0, 3)
+        nptr = nat.ptr(n) if corrector else None
+        lnptr = nat.ptr(lam_n) if (corrector and self.fric) else None
         if torch.is_tensor(dt):  # device time step (graph-captured backward passes)
             rc = self.lib.swe_adj_pointwise_dev_f32(
                 mode, nat.ptr(U), nat.ptr(k), nptr, n.shape[0], self.B, self.ny, self.nx, self.p,
@@ -127,16 +128,19 @@ class AdjointStepper:
                 mode, nat.ptr(U), nat.ptr(k), nptr, n.shape[0], self.B, self.ny, self.nx, self.p,
                 float(dt), nat.ptr(lam_out), nat.ptr(lam_U), nat.ptr(self.lam_k), lnptr,
                 nat.ptr(P_out), self.st)
-        nat.check(rc, ("adjoint corrector", "adjoint predictor", "adjoint predictor")[mode])
+        nat.check(rc, ("adjoint corrector", "adjoint predictor", "adjoint predictor",
+                       "adjoint corrector")[mode])
 
-    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n, K1=None):
+    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n, K1=None, overwrite=False):
         """lam_U += (d U_new / d U)^T lam_out and lam_n += the roughness
         adjoint (when friction is on) for the step at input state U with
         level vector lv and time step dt (a float, or a one-element device
         tensor); returns the level adjoint's partial sums
         [2, B * level_blocks] (their sum per batch member is that member's
         level adjoint).  K1, if given, is the step's stage-1 tendency kept
-        from the forward recompute (else it is recomputed here)."""
+        from the forward recompute (else it is recomputed here).  With
+        overwrite, lam_U's previous contents are ignored (lam_U = ... rather
+        than +=)."""
         K2, P, lam_k = self.K2, self.P, self.lam_k
         # recompute the step's stage intermediates (solver.py:613-646)
         if K1 is None:
@@ -145,7 +149,7 @@ class AdjointStepper:
         self._pointwise(2, U, K1, dt, None, None, None, P)
         self._tendency(P, lv, K2)
         # corrector + friction: lam_k = adjoint of k2
-        self._pointwise(0, U, K2, dt, lam_out, lam_U, lam_n, None)
+        self._pointwise(3 if overwrite else 0, U, K2, dt, lam_out, lam_U, lam_n, None)
         # spatial operator at the predictor, then the predictor: lam_k = adjoint of k1
         self._stage2(P, U, K1, lv, dt, lam_U)
         # spatial operator at the input state

@@ -4,7 +4,7 @@
 //
 // The step is S(U) -> k1, P = C(U, U + dt/2 k1), S(P) -> k2,
 // Q = C(U, U + dt k2), U' = F(Q, n).  Its adjoint runs, per step:
-//   swe_adj_pointwise_f32(mode 0): friction and corrector clean-up adjoints
+//   swe_adj_pointwise_f32(mode 0, or 3 writing lamU): friction and corrector clean-up adjoints
 //       (friction.py:12-131, solver.py:547-570) -> lamU, lam_k2, lam_n
 //   swe_adj_stage2_f32 at P:       adjoint of the spatial operator and of
 //       the predictor clean-up (solver.py:639) -> lamU, lam_k1
@@ -119,11 +119,12 @@ namespace {
 int adj_pointwise(int mode, const float* U, const float* k, const float* n, int nB, int B, int ny,
                   int nx, const swe_params* p, float dt, const float* dt_dev, const float* lam_out,
                   float* lam_U, float* lam_k, float* lam_n, float* P_out, void* stream) {
-    if (mode < 0 || mode > 2 || !U || !k || !valid_params(p) || B < 1 || ny < 1 || nx < 1)
+    if (mode < 0 || mode > 3 || !U || !k || !valid_params(p) || B < 1 || ny < 1 || nx < 1)
         return SWE_EARG;
     if (mode == 2 && !P_out) return SWE_EARG;
     if (mode != 2 && (!lam_out || !lam_U || !lam_k)) return SWE_EARG;
-    if (mode == 0 && p->apply_friction && (!n || !lam_n || (nB != 1 && nB != B))) return SWE_EARG;
+    if ((mode == 0 || mode == 3) && p->apply_friction && (!n || !lam_n || (nB != 1 && nB != B)))
+        return SWE_EARG;
     PwArgs a{};
     a.U = U;
     a.k = k;
@@ -134,7 +135,7 @@ int adj_pointwise(int mode, const float* U, const float* k, const float* n, int 
     a.ln = lam_n;
     a.P = P_out;
     a.dt = dt;
-    a.scale = mode == 0 ? dt : 0.5f * dt;
+    a.scale = (mode == 0 || mode == 3) ? dt : 0.5f * dt;
     a.dt_dev = dt_dev;
     a.B = B;
     a.nB = nB;

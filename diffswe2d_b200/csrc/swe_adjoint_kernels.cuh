@@ -65,13 +65,13 @@ struct AdjArgs {
 struct PwArgs {
     const float* U;     // step input
     const float* k;     // tendency (k2 for mode 0, k1 for mode 1)
-    const float* n;     // roughness (mode 0)
-    const float* lout;  // adjoint of the step output (mode 0) or of P (mode 1)
+    const float* n;     // roughness (modes 0, 3)
+    const float* lout;  // adjoint of the step output (modes 0, 3) or of P (mode 1)
     float* lU;          // adjoint of U, accumulated (+=)
     float* lk;          // adjoint of the tendency (written)
     float* ln;          // adjoint of the roughness field, accumulated (+=) [nB,ny,nx]
     float* P;           // mode 2: predictor output
-    float scale;        // dt (mode 0) or dt/2 (modes 1, 2)
+    float scale;        // dt (modes 0, 3) or dt/2 (modes 1, 2)
     float dt;
     const float* dt_dev;  // if set: dt read from device memory (scale derived here)
     int B, nB, ny, nx, mode, positivity, friction, friction_model;
@@ -577,7 +577,7 @@ __global__ void adj_pointwise_kernel(const PwArgs a) {
     float dt = a.dt, scale = a.scale;
     if (a.dt_dev != nullptr) {
         dt = *a.dt_dev;
-        scale = a.mode == 0 ? dt : 0.5f * dt;
+        scale = (a.mode == 0 || a.mode == 3) ? dt : 0.5f * dt;
     }
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
@@ -595,7 +595,7 @@ __global__ void adj_pointwise_kernel(const PwArgs a) {
             continue;
         }
         State lq{a.lout[o], a.lout[o + plane], a.lout[o + 2 * plane]};
-        if (a.mode == 0 && a.friction) {
+        if ((a.mode == 0 || a.mode == 3) && a.friction) {
             const State q = clean_fwd<M>(u, cand, a.kc, a.positivity != 0);
             const size_t on = (size_t)(a.nB == 1 ? 0 : b) * plane + i;
             State lqi;
@@ -607,10 +607,16 @@ __global__ void adj_pointwise_kernel(const PwArgs a) {
         }
         State lold, lcand;
         clean_bwd<M>(u, cand, lq, a.kc, a.positivity != 0, lold, lcand);
-        // cand = U + scale * k
-        a.lU[o] += lold.h + lcand.h;
-        a.lU[o + plane] += lold.hu + lcand.hu;
-        a.lU[o + 2 * plane] += lold.hv + lcand.hv;
+        // cand = U + scale * k; mode 3 writes the adjoint of U instead of adding to it
+        if (a.mode == 3) {
+            a.lU[o] = lold.h + lcand.h;
+            a.lU[o + plane] = lold.hu + lcand.hu;
+            a.lU[o + 2 * plane] = lold.hv + lcand.hv;
+        } else {
+            a.lU[o] += lold.h + lcand.h;
+            a.lU[o + plane] += lold.hu + lcand.hu;
+            a.lU[o + 2 * plane] += lold.hv + lcand.hv;
+        }
         a.lk[o] = lcand.h * scale;
         a.lk[o + plane] = lcand.hu * scale;
         a.lk[o + 2 * plane] = lcand.hv * scale;

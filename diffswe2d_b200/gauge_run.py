@@ -292,9 +292,8 @@ class GaugeRunWorkspace:
                 nat.ptr(lam_in), self.B, self.ny, self.nx, nat.ptr(self.cells), self.ngauge,
                 nat.ptr(self.g_gauge), self.n_out, self.record_cap, st)
             nat.check(rc, "gauge-run adjoint setup")
-            lam_out.zero_()
             part = stp(self.seg[i], self.lv_cur, self.dt_cur, lam_in, lam_out, self.lam_n,
-                       K1=self.seg_k1[i])
+                       K1=self.seg_k1[i], overwrite=True)
             rc = lib.swe_gauge_adjoint_post_f32(
                 nat.ptr(self.cursor), nat.ptr(self.step_code), nat.ptr(part), 2, self.B,
                 stp.level_blocks, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)

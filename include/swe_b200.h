@@ -350,7 +350,9 @@ int swe_adj_stage2_f32(const float* P, const float* U, const float* k1, const fl
  *           of k2, lam_n += adjoint of the roughness field [nB,1,ny,nx];
  *   mode 1: predictor (solver.py:639): lam_out = adjoint of P; lam_U += ...,
  *           lam_k = adjoint of k1;
- *   mode 2: forward predictor P_out = clean(U, U + dt/2 k) (for recompute).
+ *   mode 2: forward predictor P_out = clean(U, U + dt/2 k) (for recompute);
+ *   mode 3: mode 0 with lam_U written (=) instead of accumulated, for a
+ *           lam_U that starts the step's accumulation (no zeroing pass).
  */
 int swe_adj_pointwise_f32(int mode, const float* U, const float* k, const float* n, int nB, int B,
                           int ny, int nx, const swe_params* p, float dt, const float* lam_out,

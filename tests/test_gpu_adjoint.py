@@ -179,6 +179,36 @@ def test_stage2_entry_equals_spatial_then_predictor(golden, arithmetic, bed_grad
             assert _rel(a, b) <= 1e-6
 
 
+@pytest.mark.parametrize("arithmetic", ["exact", "fast"])
+def test_corrector_adjoint_overwrite_mode(golden, arithmetic):
+    """swe_adj_pointwise_f32 mode 3 (lam_U written) equals mode 0 (lam_U
+    accumulated) into a zeroed lam_U, value for value (0 + x turns a -0
+    into +0), whatever lam_U held."""
+    from diffswe2d_b200 import _native as nat
+    d = golden("adj_step")
+    cfg = SWEConfig(**STEP_CASES["walls"], constant_value=0.05)
+    m = SWE2D(_t(d["bed"]), _t(d["n"]), 0.05, 0.04, config=cfg, train_dem=False,
+              arithmetic=arithmetic)
+    lib, st, p = nat.lib(), nat.stream_handle(torch.device(DEV)), m._params()
+    U = _t(d["U"])
+    B, _, ny, nx = U.shape
+    n = m.roughness_length.detach().reshape(1, 1, ny, nx).contiguous()
+    g = torch.Generator(device="cpu").manual_seed(5)
+    k2 = (torch.randn(U.shape, generator=g) * 0.1).to(DEV)
+    lout = torch.randn(U.shape, generator=g).to(DEV)
+    outs = []
+    for mode, start in ((0, torch.zeros_like(U)), (3, torch.randn(U.shape, generator=g).to(DEV))):
+        lamU, lamk, lamn = start.clone(), torch.zeros_like(U), torch.zeros_like(n)
+        nat.check(lib.swe_adj_pointwise_f32(mode, nat.ptr(U), nat.ptr(k2), nat.ptr(n), 1, B, ny, nx, p,
+                                            2.5e-3, nat.ptr(lout), nat.ptr(lamU), nat.ptr(lamk),
+                                            nat.ptr(lamn), None, st), f"mode {mode}")
+        torch.cuda.synchronize()
+        outs.append([x.cpu().numpy() for x in (lamU, lamk, lamn)])
+    assert np.abs(outs[0][0]).max() > 0
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 def _run_model(d, requires=True, arithmetic="exact"):
     cfg = SWEConfig(boundary_left="water_level", boundary_right="wall", boundary_top="wall",
                     boundary_bottom="wall")
