@@ -583,7 +583,15 @@ class _DeviceLoop:
         self.params = params
         self.arithmetic = model.arithmetic
         self.B, self.ny, self.nx, self.levelB, self.dev = B, ny, nx, levelB, dev
-        self.graph = None
+        # graphs of `chunk` steps and of the shorter tail lengths (halving, down
+        # to 2): near the end of a call the host replays the longest one that
+        # the remaining time still fills, so that few steps run inactive
+        # (an inactive step still copies the state through)
+        self.sizes = [self.chunk]
+        while self.sizes[-1] > 2 and self.sizes[-1] % 4 == 0:
+            self.sizes.append(self.sizes[-1] // 2)
+        self.graphs = {}
+        self.dt_hint = 0.0  # mean step of the calls so far (sizes a call's first replay)
 
     def _clock_tick(self, state):
         rc = nat.lib().swe_clock_f32(
@@ -618,19 +626,29 @@ class _DeviceLoop:
         self.clock_host.copy_(torch.frombuffer(bytearray(bytes(clock)), dtype=torch.uint8))
         self.clock.copy_(self.clock_host, non_blocking=True)
         self._clock_tick(self.bufs[0])  # sets up the first step
-        if self.graph is None:
+        if not self.graphs:
             from .autotune import sweep_rows, tuned_rows_for_shape
             nat.load_kernels()
             rows = tuned_rows_for_shape(self.B, self.ny, self.nx, self.dev,
                                         arithmetic=self.arithmetic)
-            graph = torch.cuda.CUDAGraph()
-            with sweep_rows(rows), torch.cuda.graph(graph):
-                for s in range(self.chunk):
-                    self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
-            self.graph = graph
+            with sweep_rows(rows):
+                for n in self.sizes:  # even lengths: the state ends in bufs[0]
+                    graph = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(graph):
+                        for s in range(n):
+                            self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
+                    self.graphs[n] = graph
+        def size_for(left):  # the longest graph that `left` more steps fill
+            return next((m for m in self.sizes if m <= left), self.sizes[-1])
+
+        n = size_for(clock.duration / self.dt_hint) if self.dt_hint > 0 else self.chunk
         while True:
-            self.graph.replay()
+            self.graphs[n].replay()
             c = nat.SweClock.from_buffer_copy(self.clock.cpu().numpy().tobytes())
+            if c.steps > 0 and c.elapsed > 0:
+                self.dt_hint = float(c.elapsed) / c.steps
             yield self.bufs[0], c
             if c.state != nat.CLOCK_RUNNING:
                 return
+            # the steps the remaining time needs at the mean step so far
+            n = size_for((c.duration - c.elapsed) / self.dt_hint if self.dt_hint > 0 else float("inf"))
