@@ -238,6 +238,34 @@ def test_forward_device_loop_gauges_match_host_loop(golden):
     assert len(dev[0]) > 40  # more than one graph chunk
 
 
+def test_forward_device_loop_short_calls_match_host_loop(golden):
+    """Consecutive forward() calls of a few steps each (the reference's
+    per-output-interval use): after the first call the device loop sizes its
+    replays from the mean step (graphs of 32, 16, 8, 4, 2 steps); every call
+    still equals the host loop bit for bit, gauges included."""
+    d, m = _runup_model(golden)
+    m.track_gauges = True
+    m.gauge_indices = {"g0": (30, 40), "g1": (200, 380)}
+    spans = (0.03, 0.011, 0.0045, 0.07, 0.002)
+    out = []
+    for use_callback in (True, False):
+        m.reset_gauge_tracking()
+        cb = (lambda it, t, U: None) if use_callback else None
+        U, t, res = _t(d["U0"]), 0.0, []
+        with torch.no_grad():
+            for span in spans:
+                U, hmax = m(U, t_end=span, start_time=t, callback=cb)
+                t += span
+                res.append((m.last_forward_steps, _np(U), _np(hmax)))
+        out.append((res, list(m.ts_time), dict(m.ts_h)))
+    (host, ht, hh), (dev, dt_, dh) = out
+    assert [r[0] for r in host] == [r[0] for r in dev]
+    assert any(r[0] < 8 for r in dev) and any(r[0] > 8 for r in dev)
+    for a, b in zip(host, dev):
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    assert ht == dt_ and hh == dh
+
+
 def test_forward_device_loop_errors(golden):
     d, m = _runup_model(golden)
     with torch.no_grad():
