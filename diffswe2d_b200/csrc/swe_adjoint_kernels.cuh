@@ -216,6 +216,7 @@ __device__ __forceinline__ void face_dir(const AdjArgs& a, int blk, int nblk) {
 // The x faces on the first xblocks blocks, the y faces on the rest.
 template <bool BEDG, class M>
 __global__ void __launch_bounds__(ADJ_THREADS, SWE_ADJ_FACE_MINB) adj_face_kernel(const AdjArgs a, int xblocks) {
+    chain_start();
     if ((int)blockIdx.x < xblocks) face_dir<false, BEDG, M>(a, blockIdx.x, xblocks);
     else face_dir<true, BEDG, M>(a, blockIdx.x - xblocks, gridDim.x - xblocks);
 }
@@ -504,6 +505,7 @@ __device__ void friction_bwd(const State& s0, float n, float dt, int model, cons
 
 template <bool BEDG, bool PRED, class M>
 __global__ void __launch_bounds__(ADJ_THREADS, SWE_ADJ_GATHER_MINB) adj_gather_kernel(const AdjArgs a) {
+    chain_start();
     const int ny = a.ny, nx = a.nx;
     const int b = blockIdx.y;
     const long long ncell = (long long)ny * nx;
@@ -572,6 +574,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, SWE_ADJ_GATHER_MINB) adj_gather_k
 
 template <class M>
 __global__ void adj_pointwise_kernel(const PwArgs a) {
+    chain_start();
     const long long plane = (long long)a.ny * a.nx;
     const long long total = plane * a.B;
     float dt = a.dt, scale = a.scale;
@@ -635,23 +638,27 @@ template <class M>
 int launch_adj_spatial(const AdjArgs& a, int level_blocks, bool pred, cudaStream_t s) {
     const int gx = blocks_for((long long)a.B * a.ny * (a.nx + 1));
     const int gy = blocks_for((long long)a.B * (a.ny + 1) * a.nx);
-    const dim3 gg(level_blocks, a.B);
+    const dim3 gg(level_blocks, a.B), gf(gx + gy), th(ADJ_THREADS);
+    cudaError_t e;
     if (a.lbed) {
-        adj_face_kernel<true, M><<<gx + gy, ADJ_THREADS, 0, s>>>(a, gx);
-        if (pred) adj_gather_kernel<true, true, M><<<gg, ADJ_THREADS, 0, s>>>(a);
-        else adj_gather_kernel<true, false, M><<<gg, ADJ_THREADS, 0, s>>>(a);
+        e = launch_chained(adj_face_kernel<true, M>, gf, th, s, a, gx);
+        if (e == cudaSuccess)
+            e = pred ? launch_chained(adj_gather_kernel<true, true, M>, gg, th, s, a)
+                     : launch_chained(adj_gather_kernel<true, false, M>, gg, th, s, a);
     } else {
-        adj_face_kernel<false, M><<<gx + gy, ADJ_THREADS, 0, s>>>(a, gx);
-        if (pred) adj_gather_kernel<false, true, M><<<gg, ADJ_THREADS, 0, s>>>(a);
-        else adj_gather_kernel<false, false, M><<<gg, ADJ_THREADS, 0, s>>>(a);
+        e = launch_chained(adj_face_kernel<false, M>, gf, th, s, a, gx);
+        if (e == cudaSuccess)
+            e = pred ? launch_chained(adj_gather_kernel<false, true, M>, gg, th, s, a)
+                     : launch_chained(adj_gather_kernel<false, false, M>, gg, th, s, a);
     }
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 template <class M>
 int launch_adj_pointwise(const PwArgs& a, cudaStream_t s) {
-    adj_pointwise_kernel<M><<<blocks_for((long long)a.B * a.ny * a.nx), ADJ_THREADS, 0, s>>>(a);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    const cudaError_t e = launch_chained(adj_pointwise_kernel<M>, dim3(blocks_for((long long)a.B * a.ny * a.nx)),
+                                         dim3(ADJ_THREADS), s, a);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 }  // namespace

@@ -70,4 +70,36 @@ inline bool valid_params(const swe_params* p) {
            (p->arithmetic == SWE_ARITH_EXACT || p->arithmetic == SWE_ARITH_FAST);
 }
 
+// Chained launches (programmatic dependent launch, sm_90 and later).  The
+// kernels of a time step and of its adjoint form a chain in which each one
+// reads what the one before it wrote.  They are launched with
+// launch_chained(), which lets the launch of the next kernel of the stream
+// overlap the end of the current one, and each calls chain_start() before
+// its first memory access: it waits until the preceding kernel has
+// completed and its writes are visible (at once for a kernel launched the
+// ordinary way).  The kernels do not signal their dependents early: blocks
+// of the next kernel waiting beside the running ones slowed the forward
+// loop at the inversion's grid size (44.7 against 39.7 us per step).
+__device__ __forceinline__ void chain_start() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+template <typename... K, typename... A>
+inline cudaError_t launch_chained(void (*kernel)(K...), dim3 grid, dim3 block, cudaStream_t s,
+                                  A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<K>(args)...);
+}
+
 }  // namespace swe

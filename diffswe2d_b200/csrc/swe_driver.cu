@@ -39,6 +39,7 @@ __global__ void clock_kernel(swe_clock* c, uint32_t* red, const float* series_t,
                              int ny, int nx, const int32_t* gauge_cells, int ngauge, double* gauges,
                              int gauge_rows) {
     __shared__ int s_record_row;
+    chain_start();
     const int tid = threadIdx.x;
     if (tid == 0) {
         s_record_row = -1;
@@ -114,6 +115,7 @@ __global__ void run_clock_kernel(swe_run_clock* rc, uint32_t* red, const float* 
                                  float* gauge_out, float* step_dt, int32_t* step_code) {
     __shared__ int s_record;  // interval whose gauges are read from U, or -1
     __shared__ int s_level;   // interval whose level the next step uses, or -1
+    chain_start();
     const int tid = threadIdx.x;
     swe_clock* c = &rc->base;
     if (tid == 0) {
@@ -216,6 +218,7 @@ __global__ void gauge_adjoint_prep_kernel(const int32_t* cursor, const float* st
                                           float* dt_out, float* level_out, float* lam, int B, int ny,
                                           int nx, const int32_t* gauge_cells, int ngauge,
                                           const float* g_gauge, int n_out, int nsteps) {
+    chain_start();
     const int s = *cursor;
     if (s < 0 || s >= nsteps) return;  // outside the record: nothing to set up
     const int code = step_code[s];
@@ -238,6 +241,7 @@ __global__ void gauge_adjoint_post_kernel(int32_t* cursor, const int32_t* step_c
                                           int levelB, float* g_levels, int nsteps) {
     __shared__ float s_sum[32];
     __shared__ int s_step;
+    chain_start();
     if (threadIdx.x == 0) s_step = *cursor;
     __syncthreads();  // every thread has the step before thread 0 moves the cursor
     const int s = s_step;
@@ -283,10 +287,11 @@ extern "C" int swe_gauge_adjoint_prep_f32(const int32_t* cursor, const float* st
         B < 1 || ny < 1 || nx < 1 || ngauge < 0 || n_out < 1 || nsteps < 0)
         return SWE_EARG;
     if (ngauge > 0 && (!gauge_cells || !g_gauge)) return SWE_EARG;
-    gauge_adjoint_prep_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(
-        cursor, step_dt, step_code, levels, levelB, dt_out, level_out, lam, B, ny, nx, gauge_cells,
-        ngauge, g_gauge, n_out, nsteps);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    const cudaError_t e = launch_chained(gauge_adjoint_prep_kernel, dim3(1), dim3(128),
+                                         (cudaStream_t)stream, cursor, step_dt, step_code, levels,
+                                         levelB, dt_out, level_out, lam, B, ny, nx, gauge_cells, ngauge,
+                                         g_gauge, n_out, nsteps);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 extern "C" int swe_gauge_adjoint_post_f32(int32_t* cursor, const int32_t* step_code,
@@ -295,10 +300,10 @@ extern "C" int swe_gauge_adjoint_post_f32(int32_t* cursor, const int32_t* step_c
     if (!cursor || !step_code || !parts || nparts < 1 || B < 1 || blocks < 1 || !g_levels ||
         (levelB != 1 && levelB != B) || nsteps < 0)
         return SWE_EARG;
-    gauge_adjoint_post_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(cursor, step_code, parts, nparts,
-                                                                   B, blocks, levelB, g_levels,
-                                                                   nsteps);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    const cudaError_t e = launch_chained(gauge_adjoint_post_kernel, dim3(1), dim3(256),
+                                         (cudaStream_t)stream, cursor, step_code, parts, nparts, B,
+                                         blocks, levelB, g_levels, nsteps);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 extern "C" int swe_run_clock_f32(swe_run_clock* clock, uint32_t* red, const float* levels,
@@ -312,10 +317,10 @@ extern "C" int swe_run_clock_f32(swe_run_clock* clock, uint32_t* red, const floa
     if (levelB != 1 && levelB != B) return SWE_EARG;
     if (ngauge > 0 && (!gauge_cells || !gauge_out || !bed || (bedB != 1 && bedB != B)))
         return SWE_EARG;
-    run_clock_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(clock, red, levels, levelB, level_out, U,
-                                                          bed, bedB, B, ny, nx, gauge_cells, ngauge,
-                                                          gauge_out, step_dt, step_code);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    const cudaError_t e = launch_chained(run_clock_kernel, dim3(1), dim3(128), (cudaStream_t)stream,
+                                         clock, red, levels, levelB, level_out, U, bed, bedB, B, ny,
+                                         nx, gauge_cells, ngauge, gauge_out, step_dt, step_code);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 extern "C" int swe_gauge_adjoint_f32(float* lam, int B, int ny, int nx, const int32_t* gauge_cells,
@@ -337,8 +342,8 @@ extern "C" int swe_clock_f32(swe_clock* clock, uint32_t* red, const float* serie
     if (!clock || !red || nseries < 0 || ngauge < 0) return SWE_EARG;
     if (nseries > 0 && (!series_t || !series_w || !level_out)) return SWE_EARG;
     if (ngauge > 0 && gauges && (!gauge_cells || !U || ny < 1 || nx < 1)) return SWE_EARG;
-    clock_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(clock, red, series_t, series_w, nseries, level_out,
-                                                      U, ny, nx, gauge_cells, ngauge, gauges,
-                                                      gauge_rows);
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    const cudaError_t e = launch_chained(clock_kernel, dim3(1), dim3(128), (cudaStream_t)stream, clock,
+                                         red, series_t, series_w, nseries, level_out, U, ny, nx,
+                                         gauge_cells, ngauge, gauges, gauge_rows);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }

@@ -409,6 +409,7 @@ __device__ __forceinline__ void fast_tile(const StepArgs& a, int bx, int by, int
 
 template <int STAGE, int FRIC>
 __global__ void __launch_bounds__(SW_WARPS * 32, 8) fast_kernel(const StepArgs a) {
+    chain_start();
     fast_tile<STAGE, FRIC, false>(a, blockIdx.x, blockIdx.y, blockIdx.z, a.rows);
 }
 
@@ -429,14 +430,15 @@ fast_ensemble_kernel(const StepArgs* __restrict__ args, EnsCtl* ctl, int count, 
 }  // namespace
 
 int fast_launch_stages(int stage, const StepArgs& a, dim3 grid, cudaStream_t s) {
-    const int threads = SW_WARPS * 32;
-    if (stage & 1) fast_kernel<1, 0><<<grid, threads, 0, s>>>(a);
-    if (stage & 2) {
-        if (!a.friction) fast_kernel<2, 0><<<grid, threads, 0, s>>>(a);
-        else if (a.friction_model == 0) fast_kernel<2, 1><<<grid, threads, 0, s>>>(a);
-        else fast_kernel<2, 2><<<grid, threads, 0, s>>>(a);
+    const dim3 threads(SW_WARPS * 32);
+    cudaError_t e = cudaSuccess;
+    if (stage & 1) e = launch_chained(fast_kernel<1, 0>, grid, threads, s, a);
+    if ((stage & 2) && e == cudaSuccess) {
+        if (!a.friction) e = launch_chained(fast_kernel<2, 0>, grid, threads, s, a);
+        else if (a.friction_model == 0) e = launch_chained(fast_kernel<2, 1>, grid, threads, s, a);
+        else e = launch_chained(fast_kernel<2, 2>, grid, threads, s, a);
     }
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 int fast_launch_ensemble(int friction, int blocks, const StepArgs* args, EnsCtl* ctl, int count,

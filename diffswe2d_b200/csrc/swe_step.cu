@@ -424,6 +424,7 @@ __device__ __forceinline__ void sweep_tile(const StepArgs& a, int bx, int by, in
 // six blocks (80 registers); ten blocks spill too much.
 template <int STAGE, int FRIC>
 __global__ void __launch_bounds__(SW_WARPS * 32, 8) sweep_kernel(const StepArgs a) {
+    chain_start();
     sweep_tile<STAGE, FRIC, false>(a, blockIdx.x, blockIdx.y, blockIdx.z, a.rows);
 }
 
@@ -562,7 +563,8 @@ extern "C" int swe_spatial_operator_f32(const float* U, const float* bed, int B,
     // the stage-1 kernel of the step computes exactly this (tendency + maxima)
     if (p->arithmetic == SWE_ARITH_FAST) return fast_launch_stages(1, a, sweep_grid_of(a), s);
     if (use_tiled_kernels()) stage_kernel<1><<<grid_of(a), NT, 0, s>>>(a);
-    else sweep_kernel<1, 0><<<sweep_grid_of(a), SW_WARPS * 32, 0, s>>>(a);
+    else if (launch_chained(sweep_kernel<1, 0>, sweep_grid_of(a), dim3(SW_WARPS * 32), s, a) != cudaSuccess)
+        return SWE_ECUDA;
     return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
@@ -603,22 +605,24 @@ int launch_step(int stage, const float* U, const float* bed, int bedB, const flo
     if ((stage & 1) && !clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
         return SWE_ECUDA;
     if (fast) return fast_launch_stages(stage, a, g, s);
+    const dim3 th(SW_WARPS * 32);
+    cudaError_t e = cudaSuccess;
     if (stage & 1) {
         if (tiled) stage_kernel<1><<<g, NT, 0, s>>>(a);
-        else sweep_kernel<1, 0><<<g, SW_WARPS * 32, 0, s>>>(a);
+        else e = launch_chained(sweep_kernel<1, 0>, g, th, s, a);
     }
-    if (stage & 2) {
+    if ((stage & 2) && e == cudaSuccess) {
         if (tiled) {
             stage_kernel<2><<<g, NT, 0, s>>>(a);
         } else if (!a.friction) {
-            sweep_kernel<2, 0><<<g, SW_WARPS * 32, 0, s>>>(a);
+            e = launch_chained(sweep_kernel<2, 0>, g, th, s, a);
         } else if (a.friction_model == 0) {
-            sweep_kernel<2, 1><<<g, SW_WARPS * 32, 0, s>>>(a);
+            e = launch_chained(sweep_kernel<2, 1>, g, th, s, a);
         } else {
-            sweep_kernel<2, 2><<<g, SW_WARPS * 32, 0, s>>>(a);
+            e = launch_chained(sweep_kernel<2, 2>, g, th, s, a);
         }
     }
-    return cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? SWE_OK : SWE_ECUDA;
 }
 
 }  // namespace
