@@ -154,6 +154,8 @@ _SIGNATURES = {
     "swe_gauge_adjoint_f32": [_P, _I, _I, _I, _P, _I, _P, _I, _I, _P],
     "swe_step_clocked_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I,
                              _P, _P, _I, _I, _P, _P, _P, _P, _P],
+    "swe_step_clocked_k2_f32": [_I, _P, _P, _I, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P,
+                                _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P],
     "swe_adj_spatial_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _P, _P,
                             _P, _P, _I, _P],
     "swe_adj_spatial_bed_f32": [_P, _P, _I, _I, _I, _I, ctypes.POINTER(SweParams), _P, _I, _P, _P,

@@ -131,23 +131,25 @@ class AdjointStepper:
         nat.check(rc, ("adjoint corrector", "adjoint predictor", "adjoint predictor",
                        "adjoint corrector")[mode])
 
-    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n, K1=None, overwrite=False):
+    def __call__(self, U, lv, dt, lam_out, lam_U, lam_n, K1=None, overwrite=False, K2=None):
         """lam_U += (d U_new / d U)^T lam_out and lam_n += the roughness
         adjoint (when friction is on) for the step at input state U with
         level vector lv and time step dt (a float, or a one-element device
         tensor); returns the level adjoint's partial sums
         [2, B * level_blocks] (their sum per batch member is that member's
         level adjoint).  K1, if given, is the step's stage-1 tendency kept
-        from the forward recompute (else it is recomputed here).  With
-        overwrite, lam_U's previous contents are ignored (lam_U = ... rather
-        than +=)."""
-        K2, P, lam_k = self.K2, self.P, self.lam_k
+        from the forward recompute (else it is recomputed here); K2 likewise
+        the step's stage-2 tendency.  With overwrite, lam_U's previous
+        contents are ignored (lam_U = ... rather than +=)."""
+        P, lam_k = self.P, self.lam_k
         # recompute the step's stage intermediates (solver.py:613-646)
         if K1 is None:
             K1 = self.K1
             self._tendency(U, lv, K1)
         self._pointwise(2, U, K1, dt, None, None, None, P)
-        self._tendency(P, lv, K2)
+        if K2 is None:
+            K2 = self.K2
+            self._tendency(P, lv, K2)
         # corrector + friction: lam_k = adjoint of k2
         self._pointwise(3 if overwrite else 0, U, K2, dt, lam_out, lam_U, lam_n, None)
         # spatial operator at the predictor, then the predictor: lam_k = adjoint of k1

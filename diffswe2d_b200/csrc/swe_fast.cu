@@ -351,6 +351,11 @@ __device__ __forceinline__ void fast_tile(const StepArgs& a, int bx, int by, int
                             a.tend[oo + plane] = r1;
                             a.tend[oo + 2 * plane] = r2;
                         } else {
+                            if (a.k2_out != nullptr) {
+                                a.k2_out[oo] = r0;
+                                a.k2_out[oo + plane] = r1;
+                                a.k2_out[oo + 2 * plane] = r2;
+                            }
                             const State u{ld_state<CG>(a.U + oo), ld_state<CG>(a.U + oo + plane),
                                           ld_state<CG>(a.U + oo + 2 * plane)};
                             State upd = fclean(u, r0, r1, r2, dt, k.eps, k.dry, a.positivity);

@@ -384,6 +384,11 @@ __device__ __forceinline__ void sweep_tile(const StepArgs& a, int bx, int by, in
                         a.tend[oo + plane] = r.r1;
                         a.tend[oo + 2 * plane] = r.r2;
                     } else {
+                        if (a.k2_out != nullptr) {
+                            a.k2_out[oo] = r.r0;
+                            a.k2_out[oo + plane] = r.r1;
+                            a.k2_out[oo + 2 * plane] = r.r2;
+                        }
                         const State u = um2;
                         const State cand{u.h + dt * r.r0, u.hu + dt * r.r1, u.hv + dt * r.r2};
                         State upd = clean_and_limit(u, cand, kc, a.positivity != 0);
@@ -575,7 +580,7 @@ int launch_step(int stage, const float* U, const float* bed, int bedB, const flo
                 int ny, int nx, const swe_params* p, const float* level, int levelB, float max_dt,
                 const swe_clock* clk, const float* rain, int rain_mode, int rain_batch,
                 const float* infil, int infil_mode, int infil_batch, float* scratch_k, uint32_t* red,
-                float* U_out, float* hmax, void* stream) {
+                float* U_out, float* hmax, void* stream, float* k2_out = nullptr) {
     StepArgs a{};
     if (stage != 1 && stage != 2 && stage != 3) return SWE_EARG;
     if (!fill_common(a, U, bed, B, bedB, ny, nx, p, level, levelB)) return SWE_EARG;
@@ -597,9 +602,11 @@ int launch_step(int stage, const float* U, const float* bed, int bedB, const flo
     a.max_dt = max_dt;
     a.clk = clk;
     a.hmax = hmax;
+    a.k2_out = k2_out;
     cudaStream_t s = (cudaStream_t)stream;
     const bool fast = p->arithmetic == SWE_ARITH_FAST;
     const bool tiled = !fast && use_tiled_kernels();
+    if (k2_out && tiled) return SWE_EARG;  // the tiled IEEE kernels do not write k2
     const dim3 g = tiled ? grid_of(a) : sweep_grid_of(a);
     // A clocked step's reduction words are cleared by swe_clock_f32.
     if ((stage & 1) && !clk && cudaMemsetAsync(red, 0, SWE_RED_WORDS * sizeof(uint32_t), s) != cudaSuccess)
@@ -661,6 +668,18 @@ extern "C" int swe_step_clocked_f32(int stage, const float* U, const float* bed,
     return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, 0.0f, clock, nullptr,
                        SWE_FORCING_NONE, 1, infil, infil_mode, infil_batch, scratch_k, red, U_out, hmax,
                        stream);
+}
+
+extern "C" int swe_step_clocked_k2_f32(int stage, const float* U, const float* bed, int bedB,
+                                       const float* n, int nB, int B, int ny, int nx,
+                                       const swe_params* p, const float* level, int levelB,
+                                       const swe_clock* clock, const float* infil, int infil_mode,
+                                       int infil_batch, float* scratch_k, uint32_t* red,
+                                       float* U_out, float* hmax, float* k2_out, void* stream) {
+    if (!clock || !k2_out || !(stage & 2)) return SWE_EARG;
+    return launch_step(stage, U, bed, bedB, n, nB, B, ny, nx, p, level, levelB, 0.0f, clock, nullptr,
+                       SWE_FORCING_NONE, 1, infil, infil_mode, infil_batch, scratch_k, red, U_out, hmax,
+                       stream, k2_out);
 }
 
 extern "C" int swe_step_f32(const float* U, const float* bed, int bedB, const float* n, int nB,

@@ -33,6 +33,7 @@ struct StepArgs {
     uint32_t* red;
     const swe_clock* clk;  // device clock of forward(), or null for a plain step
     float* hmax;           // running max depth [B,ny,nx], or null
+    float* k2_out;         // stage 2: its tendency k2 [B,3,ny,nx], or null
     int rows;              // output rows per sweep tile
     float max_dt, cval;
     int B, bedB, nB, levelB, ny, nx;

@@ -40,11 +40,11 @@ from .adjoint import AdjointStepper, bed_input
 GRAPH_STEPS = 32
 CHECKPOINT_EVERY = 128
 # Kernels of this library per solver step: forward (stage 1, stage 2, the
-# run clock) and adjoint with the stage-1 tendency kept (cursor set-up,
-# predictor, k2 tendency, corrector adjoint, stage-2 spatial + predictor
-# adjoint (2), stage-1 spatial adjoint (2), cursor finish).
+# run clock) and adjoint with both stage tendencies kept (cursor set-up,
+# predictor, corrector adjoint, stage-2 spatial + predictor adjoint (2),
+# stage-1 spatial adjoint (2), cursor finish).
 FORWARD_KERNELS_PER_STEP = 3
-ADJOINT_KERNELS_PER_STEP = 9
+ADJOINT_KERNELS_PER_STEP = 8
 
 
 class GaugeRunWorkspace:
@@ -96,9 +96,9 @@ class GaugeRunWorkspace:
         self.stepper = None
         # full-trajectory storage (None: when free device memory allows)
         self.store_mode = store_states
-        self.ring = self.ring_k1 = None
+        self.ring = self.ring_k1 = self.ring_k2 = None
         self.fwd_store_graph = None
-        self.store, self.store_k1 = [], []
+        self.store, self.store_k1, self.store_k2 = [], [], []
         self.stored = False
         from .autotune import tuned_rows_for_shape
         self.rows = tuned_rows_for_shape(B, ny, nx, dev, arithmetic=model.arithmetic)
@@ -112,15 +112,19 @@ class GaugeRunWorkspace:
             nat.ptr(self.step_code), nat.stream_handle(self.dev))
         nat.check(rc, "gauge-run clock")
 
-    def _step(self, src, dst, k1=None):
+    def _step(self, src, dst, k1=None, k2=None):
         """One clocked step src -> dst; its stage-1 tendency goes to k1 (the
-        shared scratch if None) and the clock advances."""
+        shared scratch if None), its stage-2 tendency to k2 (if given) and
+        the clock advances."""
         k1 = self.scratch if k1 is None else k1
-        rc = nat.lib().swe_step_clocked_f32(
-            3, nat.ptr(src), nat.ptr(self.bed), self.bed.shape[0], nat.ptr(self.n), self.n.shape[0],
-            self.B, self.ny, self.nx, self.params, nat.ptr(self.lv), self.levelB, nat.ptr(self.clock),
-            None, nat.FORCING_NONE, 1, nat.ptr(k1), nat.ptr(self.red), nat.ptr(dst), None,
-            nat.stream_handle(self.dev))
+        args = (3, nat.ptr(src), nat.ptr(self.bed), self.bed.shape[0], nat.ptr(self.n), self.n.shape[0],
+                self.B, self.ny, self.nx, self.params, nat.ptr(self.lv), self.levelB,
+                nat.ptr(self.clock), None, nat.FORCING_NONE, 1, nat.ptr(k1), nat.ptr(self.red),
+                nat.ptr(dst), None)
+        if k2 is None:
+            rc = nat.lib().swe_step_clocked_f32(*args, nat.stream_handle(self.dev))
+        else:
+            rc = nat.lib().swe_step_clocked_k2_f32(*args, nat.ptr(k2), nat.stream_handle(self.dev))
         nat.check(rc, "gauge-run step")
         self._tick(dst)
 
@@ -173,11 +177,12 @@ class GaugeRunWorkspace:
             from .autotune import sweep_rows
             self.ring = torch.empty((self.G,) + tuple(self.bufs[0].shape), device=self.dev)
             self.ring_k1 = torch.empty_like(self.ring)
+            self.ring_k2 = torch.empty_like(self.ring)
             g = torch.cuda.CUDAGraph()
             with sweep_rows(self.rows), torch.cuda.graph(g):
                 for s in range(self.G):
                     self._step(self.bufs[0] if s == 0 else self.ring[s - 1], self.ring[s],
-                               self.ring_k1[s])
+                               self.ring_k1[s], self.ring_k2[s])
                 self.bufs[0].copy_(self.ring[self.G - 1])
             self.fwd_store_graph = g
         per_ckpt = self.k // self.G
@@ -209,19 +214,21 @@ class GaugeRunWorkspace:
 
     # ------------------------------------------------------------ backward
     def _keep_replay(self, r: int) -> bool:
-        """Copy replay r's step outputs and tendencies into the store; False
-        (stop storing) when the store would leave too little device memory
-        or storage is switched off."""
+        """Copy replay r's step outputs and stage tendencies into the store;
+        False (stop storing) when the store would leave too little device
+        memory or storage is switched off."""
         if r == len(self.store):
-            need = 2 * self.ring.numel() * 4
+            need = 3 * self.ring.numel() * 4
             if self.store_mode is None:
                 free, total = torch.cuda.mem_get_info(self.dev)
                 if free - need < max(8 << 30, int(0.15 * total)):
                     return False
             self.store.append(torch.empty_like(self.ring))
             self.store_k1.append(torch.empty_like(self.ring_k1))
+            self.store_k2.append(torch.empty_like(self.ring_k2))
         self.store[r].copy_(self.ring)
         self.store_k1[r].copy_(self.ring_k1)
+        self.store_k2[r].copy_(self.ring_k2)
         return True
 
     def _copy_steps(self, dst, d0: int, chunks, s0: int, n: int):
@@ -234,24 +241,27 @@ class GaugeRunWorkspace:
             d0, s0, n = d0 + m, s0 + m, n - m
 
     def _stored_segment(self, j: int, s0: int, s1: int):
-        """The segment's states and stage-1 tendencies copied from the store."""
+        """The segment's states and stage tendencies copied from the store."""
         self._alloc_segment()
         n = s1 - s0
         self.seg[0].copy_(self.ckpts[j])
         if n > 1:
             self._copy_steps(self.seg, 1, self.store, s0, n - 1)  # outputs of s0 .. s1-2
         self._copy_steps(self.seg_k1, 0, self.store_k1, s0, n)
+        self._copy_steps(self.seg_k2, 0, self.store_k2, s0, n)
 
     def _alloc_segment(self):
         if self.seg is None:
             shape = tuple(self.bufs[0].shape)
             self.seg = torch.empty((self.k + 1,) + shape, device=self.dev)
             self.seg_k1 = torch.empty((self.k,) + shape, device=self.dev)
+            self.seg_k2 = torch.empty((self.k,) + shape, device=self.dev)
 
     def _recompute_segment(self, j: int, s0: int, s1: int):
         """States entering steps s0 .. s1-1 into self.seg[0 .. s1-s0-1] and
-        their stage-1 tendencies into self.seg_k1 (the adjoint reuses them:
-        the same kernel on the same state and level gives the same bits)."""
+        their stage tendencies into self.seg_k1 / self.seg_k2 (the adjoint
+        reuses them: the same kernels on the same state and level give the
+        same bits)."""
         self._alloc_segment()
         self.seg[0].copy_(self.ckpts[j])
         self._set_clock(replay=1, replay_end=s1, steps=s0, active=0)
@@ -262,7 +272,7 @@ class GaugeRunWorkspace:
             g = torch.cuda.CUDAGraph()
             with sweep_rows(self.rows), torch.cuda.graph(g):
                 for i in range(self.k):
-                    self._step(self.seg[i], self.seg[i + 1], self.seg_k1[i])
+                    self._step(self.seg[i], self.seg[i + 1], self.seg_k1[i], self.seg_k2[i])
             self.replay_graph = g
         self.replay_graph.replay()
 
@@ -293,7 +303,7 @@ class GaugeRunWorkspace:
                 nat.ptr(self.g_gauge), self.n_out, self.record_cap, st)
             nat.check(rc, "gauge-run adjoint setup")
             part = stp(self.seg[i], self.lv_cur, self.dt_cur, lam_in, lam_out, self.lam_n,
-                       K1=self.seg_k1[i], overwrite=True)
+                       K1=self.seg_k1[i], K2=self.seg_k2[i], overwrite=True)
             rc = lib.swe_gauge_adjoint_post_f32(
                 nat.ptr(self.cursor), nat.ptr(self.step_code), nat.ptr(part), 2, self.B,
                 stp.level_blocks, self.levelB, nat.ptr(self.g_levels), self.record_cap, st)

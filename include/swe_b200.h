@@ -285,6 +285,19 @@ int swe_step_clocked_f32(int stage, const float* U, const float* bed, int bedB, 
                          int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
                          float* hmax, void* stream);
 
+/*
+ * swe_step_clocked_f32 (stage 2 or 3) that also writes stage 2's tendency
+ * k2 = rhs(P) at the predictor P (solver.py:641) into k2_out [B,3,ny,nx],
+ * as the step computes it, for an adjoint pass that then need not
+ * re-evaluate it.  Steps the clock marks inactive leave k2_out untouched.
+ * SWE_EARG with the tiled IEEE kernels (SWE_STEP_KERNEL=tiled).
+ */
+int swe_step_clocked_k2_f32(int stage, const float* U, const float* bed, int bedB, const float* n,
+                            int nB, int B, int ny, int nx, const swe_params* p, const float* level,
+                            int levelB, const swe_clock* clock, const float* infil, int infil_mode,
+                            int infil_batch, float* scratch_k, uint32_t* red, float* U_out,
+                            float* hmax, float* k2_out, void* stream);
+
 /* ---------------------------------------------------------------------
  * Adjoint of the step (the reference's autograd gradient through
  * SWE2D.step, src/solver.py:572-663, with dt detached as in :626).  The
