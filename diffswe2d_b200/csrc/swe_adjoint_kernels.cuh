@@ -6,7 +6,7 @@
 // The spatial-operator adjoint is two launches: adj_face_kernel, one thread
 // per face (x faces, then y faces, in one grid), computes the face's reverse
 // mode (swe_adjoint.cuh) and writes its contributions to its four stencil
-// cells into a face-indexed buffer; adj_gather_kernel, one thread per cell,
+// cells into face-record planes; adj_gather_kernel, one thread per cell,
 // sums them in a fixed order and folds the adjoints of ghost cells back into
 // the interior cells and boundary level they were made from (the adjoint of
 // add_ghost_cells, src/boundary.py:150-413), and, for stage 2, goes on
@@ -64,10 +64,10 @@ struct AdjArgs {
 
 struct PwArgs {
     const float* U;     // step input
-    const float* k;     // tendency (k2 for mode 0, k1 for mode 1)
+    const float* k;     // tendency (k2 for modes 0 and 3, k1 for modes 1 and 2)
     const float* n;     // roughness (modes 0, 3)
     const float* lout;  // adjoint of the step output (modes 0, 3) or of P (mode 1)
-    float* lU;          // adjoint of U, accumulated (+=)
+    float* lU;          // adjoint of U, accumulated (+=; written in mode 3)
     float* lk;          // adjoint of the tendency (written)
     float* ln;          // adjoint of the roughness field, accumulated (+=) [nB,ny,nx]
     float* P;           // mode 2: predictor output
