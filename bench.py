@@ -432,9 +432,13 @@ def end_to_end(sc, args, dev, world, arithmetic, dt_probe):
 
     nbytes = host_in.numel() * 4
     ms_seq, counts_seq = timed(sequential)
-    ms, counts = timed(pipelined)
+    runs = [timed(pipelined) for _ in range(3)]  # the median of three: copies share the host's PCIe
+    rates = [world * ny * nx * sum(c) / (m * 1e-3) / 1e6 for m, c in runs]
+    order = sorted(range(3), key=lambda r: rates[r])
+    ms, counts = runs[order[1]]
     steps, steps_seq = sum(counts), sum(counts_seq)
     return {"value": world * ny * nx * steps / (ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+            "pipelined_values": rates,
             "h2d_bytes_per_step": nbytes * len(counts) / steps,
             "d2h_bytes_per_step": nbytes * len(counts) / steps,
             "h2d_bytes_per_call": nbytes, "d2h_bytes_per_call": nbytes,
@@ -442,8 +446,9 @@ def end_to_end(sc, args, dev, world, arithmetic, dt_probe):
             "sequential_value": world * ny * nx * steps_seq / (ms_seq * 1e-3) / 1e6,
             "api": "SWE2D.forward(U0 copied from pinned host, t_end = about 100 CFL steps; "
                    "device-driven time loop) + state copied back to pinned host, per call, 6 calls "
-                   "with the copies on a copy stream overlapping the neighbouring calls' compute "
-                   "(sequential_value: 3 calls, copy in / forward / copy out one after another); "
+                   "with the copies on a copy stream overlapping the neighbouring calls' compute, "
+                   "the median of three such runs (pipelined_values: all three; sequential_value: 3 "
+                   "calls, copy in / forward / copy out one after another); "
                    "bytes per step are the per-call copies divided by the solver steps of the call"}
 
 
