@@ -431,7 +431,8 @@ def end_to_end(sc, args, dev, world, arithmetic, dt_probe):
         return counts
 
     nbytes = host_in.numel() * 4
-    ms_seq, counts_seq = timed(sequential)
+    seq_runs = sorted((timed(sequential) for _ in range(3)), key=lambda r: r[0])
+    ms_seq, counts_seq = seq_runs[1]
     runs = [timed(pipelined) for _ in range(3)]  # the median of three: copies share the host's PCIe
     rates = [world * ny * nx * sum(c) / (m * 1e-3) / 1e6 for m, c in runs]
     order = sorted(range(3), key=lambda r: rates[r])
@@ -447,8 +448,8 @@ def end_to_end(sc, args, dev, world, arithmetic, dt_probe):
             "api": "SWE2D.forward(U0 copied from pinned host, t_end = about 100 CFL steps; "
                    "device-driven time loop) + state copied back to pinned host, per call, 6 calls "
                    "with the copies on a copy stream overlapping the neighbouring calls' compute, "
-                   "the median of three such runs (pipelined_values: all three; sequential_value: 3 "
-                   "calls, copy in / forward / copy out one after another); "
+                   "the median of three such runs (pipelined_values: all three; sequential_value: the "
+                   "median of three runs of 3 calls, copy in / forward / copy out one after another); "
                    "bytes per step are the per-call copies divided by the solver steps of the call"}
 
 
