@@ -96,8 +96,10 @@ class GaugeRunWorkspace:
         self.stepper = None
         # full-trajectory storage (None: when free device memory allows)
         self.store_mode = store_states
-        self.ring = self.ring_k1 = self.ring_k2 = None
-        self.fwd_store_graph = None
+        self.rings = None  # two (state, k1, k2) rings of graph_steps items, used alternately
+        self.copy_stream = None
+        self.ring_done = self.ring_free = None
+        self.fwd_store_graphs = None
         self.store, self.store_k1, self.store_k2 = [], [], []
         self.stored = False
         from .autotune import tuned_rows_for_shape
@@ -173,18 +175,25 @@ class GaugeRunWorkspace:
                     self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
             self.fwd_graph = g
         storing = self.store_mode is not False
-        if storing and self.fwd_store_graph is None:
+        if storing and self.fwd_store_graphs is None:
+            # two rings: replay r writes ring r % 2 while the copy stream moves
+            # ring (r - 1) % 2 into the store
             from .autotune import sweep_rows
-            self.ring = torch.empty((self.G,) + tuple(self.bufs[0].shape), device=self.dev)
-            self.ring_k1 = torch.empty_like(self.ring)
-            self.ring_k2 = torch.empty_like(self.ring)
-            g = torch.cuda.CUDAGraph()
-            with sweep_rows(self.rows), torch.cuda.graph(g):
-                for s in range(self.G):
-                    self._step(self.bufs[0] if s == 0 else self.ring[s - 1], self.ring[s],
-                               self.ring_k1[s], self.ring_k2[s])
-                self.bufs[0].copy_(self.ring[self.G - 1])
-            self.fwd_store_graph = g
+            shape = (self.G,) + tuple(self.bufs[0].shape)
+            self.rings = [tuple(torch.empty(shape, device=self.dev) for _ in range(3)) for _ in range(2)]
+            self.copy_stream = torch.cuda.Stream(self.dev)
+            self.ring_done = [torch.cuda.Event() for _ in range(2)]
+            self.ring_free = [torch.cuda.Event() for _ in range(2)]
+            graphs = []
+            for st, k1, k2 in self.rings:
+                g = torch.cuda.CUDAGraph()
+                with sweep_rows(self.rows), torch.cuda.graph(g):
+                    for s in range(self.G):
+                        self._step(self.bufs[0] if s == 0 else st[s - 1], st[s], k1[s], k2[s])
+                    self.bufs[0].copy_(st[self.G - 1])
+                graphs.append(g)
+            self.fwd_store_graphs = graphs
+        cur = torch.cuda.current_stream(self.dev)
         per_ckpt = self.k // self.G
         replay = 0
         while True:
@@ -193,14 +202,22 @@ class GaugeRunWorkspace:
                 if j == len(self.ckpts):
                     self.ckpts.append(torch.empty_like(self.bufs[0]))
                 self.ckpts[j].copy_(self.bufs[0])
-            (self.fwd_store_graph if storing else self.fwd_graph).replay()
-            self.kernel_launches += self.G * FORWARD_KERNELS_PER_STEP
             if storing:
-                storing = self._keep_replay(replay)
+                i = replay % 2
+                if replay >= 2:
+                    cur.wait_event(self.ring_free[i])  # its previous contents are in the store
+                self.fwd_store_graphs[i].replay()
+                self.ring_done[i].record(cur)
+                storing = self._keep_replay(replay, i)
+            else:
+                self.fwd_graph.replay()
+            self.kernel_launches += self.G * FORWARD_KERNELS_PER_STEP
             replay += 1
             c = self._read_clock()
             if c.base.state != nat.CLOCK_RUNNING:
                 break
+        if self.copy_stream is not None:
+            cur.wait_stream(self.copy_stream)  # the store is complete before the backward pass
         self.stored = storing
         if c.base.state == nat.CLOCK_FAILED:
             self.model._raise_on_status(int(c.base.dt_status), float(c.base.last_dt))
@@ -213,22 +230,27 @@ class GaugeRunWorkspace:
         return self.gauge_out[..., : self.ngauge], self.bufs[0]
 
     # ------------------------------------------------------------ backward
-    def _keep_replay(self, r: int) -> bool:
-        """Copy replay r's step outputs and stage tendencies into the store;
-        False (stop storing) when the store would leave too little device
-        memory or storage is switched off."""
+    def _keep_replay(self, r: int, i: int) -> bool:
+        """Copy replay r's step outputs and stage tendencies (ring i) into
+        the store on the copy stream; False (stop storing) when the store
+        would leave too little device memory or storage is switched off."""
+        ring = self.rings[i]
         if r == len(self.store):
-            need = 3 * self.ring.numel() * 4
+            need = 3 * ring[0].numel() * 4
             if self.store_mode is None:
                 free, total = torch.cuda.mem_get_info(self.dev)
                 if free - need < max(8 << 30, int(0.15 * total)):
                     return False
-            self.store.append(torch.empty_like(self.ring))
-            self.store_k1.append(torch.empty_like(self.ring_k1))
-            self.store_k2.append(torch.empty_like(self.ring_k2))
-        self.store[r].copy_(self.ring)
-        self.store_k1[r].copy_(self.ring_k1)
-        self.store_k2[r].copy_(self.ring_k2)
+            self.store.append(torch.empty_like(ring[0]))
+            self.store_k1.append(torch.empty_like(ring[1]))
+            self.store_k2.append(torch.empty_like(ring[2]))
+        cs = self.copy_stream
+        cs.wait_event(self.ring_done[i])
+        with torch.cuda.stream(cs):
+            for dst, src in zip((self.store[r], self.store_k1[r], self.store_k2[r]), ring):
+                dst.copy_(src)
+                dst.record_stream(cs)
+            self.ring_free[i].record(cs)
         return True
 
     def _copy_steps(self, dst, d0: int, chunks, s0: int, n: int):
