@@ -15,13 +15,15 @@ state after each call, autograd through everything (optionally
   on the device, every step's dt and interval are recorded on the device,
   and the state is copied to a checkpoint every ``checkpoint_every`` steps.
   No host synchronisation inside the run except one clock read per replay.
-* backward: segment by segment in reverse, the segment's states are
-  recomputed from its checkpoint in replay mode (bit for bit the forward's
-  states), then the hand-written step adjoint runs in reverse over the
-  segment with the gauge cotangents injected at the end of each interval.
-  When the whole trajectory fits in device memory (``store_states``, decided
-  by free memory by default), the forward pass keeps every step's output
-  state and stage-1 tendency instead, and the backward pass copies a
+* backward: segment by segment in reverse, the segment's states and both
+  stage tendencies are recomputed from its checkpoint in replay mode (bit
+  for bit the forward's), then the hand-written step adjoint runs in
+  reverse over the segment with the gauge cotangents injected at the end of
+  each interval (it re-evaluates only the predictor).  When the whole
+  trajectory fits in device memory (``store_states``, decided by free
+  memory by default), the forward pass keeps every step's output state and
+  stage tendencies instead (its graphs write two alternating rings, copied
+  into the store on a copy stream), and the backward pass copies a
   segment's states into place rather than recomputing them.
 
 Gradients flow to the initial state, the per-interval levels and the
