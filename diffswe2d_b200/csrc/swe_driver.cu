@@ -42,59 +42,63 @@ __global__ void clock_kernel(swe_clock* c, uint32_t* red, const float* series_t,
     chain_start();
     const int tid = threadIdx.x;
     if (tid == 0) {
+        // read at once into registers, updated there, written back in one go
+        swe_clock cl = *c;
+        const uint32_t red_status = red[2], red_dt = red[3];
         s_record_row = -1;
-        if (c->active) {
+        if (cl.active) {
             // The step that just ran (solver.py:627-632, :765-768).
-            const uint32_t st = red[2];
-            const float dt = __uint_as_float(red[3]);
+            const uint32_t st = red_status;
+            const float dt = __uint_as_float(red_dt);
             if (st & (SWE_S_NONFINITE_STATE | SWE_S_NONFINITE_DT | SWE_S_NONPOSITIVE_DT)) {
-                c->state = SWE_CLOCK_FAILED;
-                c->dt_status = st;
-                c->last_dt = dt;
-                c->active = 0;
+                cl.state = SWE_CLOCK_FAILED;
+                cl.dt_status = st;
+                cl.last_dt = dt;
+                cl.active = 0;
             } else {
-                double elapsed = c->elapsed + (double)dt;
-                if (elapsed > c->duration && elapsed - c->duration <= c->tolerance) elapsed = c->duration;
-                c->elapsed = elapsed;
-                c->last_dt = dt;
-                c->steps += 1;
+                double elapsed = cl.elapsed + (double)dt;
+                if (elapsed > cl.duration && elapsed - cl.duration <= cl.tolerance) elapsed = cl.duration;
+                cl.elapsed = elapsed;
+                cl.last_dt = dt;
+                cl.steps += 1;
                 if (gauges && gauge_rows > 0) {
-                    const int row = (c->steps - 1) % gauge_rows;
-                    gauges[(size_t)row * (2 + ngauge)] = c->start + elapsed;
+                    const int row = (cl.steps - 1) % gauge_rows;
+                    gauges[(size_t)row * (2 + ngauge)] = cl.start + elapsed;
                     gauges[(size_t)row * (2 + ngauge) + 1] = (double)dt;
                     s_record_row = row;
                 }
             }
         }
-        if (c->state == SWE_CLOCK_RUNNING) {
+        if (cl.state == SWE_CLOCK_RUNNING) {
             // The next step (solver.py:741-760).
             // The loop runs out of iterations before it checks the remaining
             // time again, so max_steps is tested first.
-            const double remaining = c->duration - c->elapsed;
-            if (c->steps >= c->max_steps) {
-                c->state = SWE_CLOCK_MAXSTEPS;
-                c->active = 0;
-            } else if (remaining <= c->tolerance) {
-                c->state = SWE_CLOCK_DONE;
-                c->active = 0;
+            const double remaining = cl.duration - cl.elapsed;
+            if (cl.steps >= cl.max_steps) {
+                cl.state = SWE_CLOCK_MAXSTEPS;
+                cl.active = 0;
+            } else if (remaining <= cl.tolerance) {
+                cl.state = SWE_CLOCK_DONE;
+                cl.active = 0;
             } else {
                 double step_max_dt = remaining;
-                if (c->max_dt_cap > 0.0 && c->max_dt_cap < remaining) step_max_dt = c->max_dt_cap;
-                c->max_dt = (float)step_max_dt;
-                const double current = c->start + c->elapsed;
+                if (cl.max_dt_cap > 0.0 && cl.max_dt_cap < remaining) step_max_dt = cl.max_dt_cap;
+                cl.max_dt = (float)step_max_dt;
+                const double current = cl.start + cl.elapsed;
                 if (nseries > 0) {
                     const float lev = interpolate_level(series_t, series_w, nseries, (float)current);
-                    c->level = lev;
+                    cl.level = lev;
                     level_out[0] = lev;
                 }
                 red[0] = 0u;
                 red[1] = 0u;
                 red[2] = 0u;
-                c->active = 1;
+                cl.active = 1;
             }
         } else {
-            c->active = 0;
+            cl.active = 0;
         }
+        *c = cl;
     }
     __syncthreads();
     const int row = s_record_row;
@@ -117,74 +121,80 @@ __global__ void run_clock_kernel(swe_run_clock* rc, uint32_t* red, const float* 
     __shared__ int s_level;   // interval whose level the next step uses, or -1
     chain_start();
     const int tid = threadIdx.x;
-    swe_clock* c = &rc->base;
     if (tid == 0) {
+        // the clock and the step's status and dt are read at once into
+        // registers, updated there and written back in one go (a chain of
+        // dependent global accesses on one thread is the kernel's latency)
+        swe_run_clock r = *rc;
+        swe_clock& cl = r.base;
+        const uint32_t red_status = red[2], red_dt = red[3];
         s_record = -1;
         s_level = -1;
-        if (rc->replay) {
-            if (c->active) c->steps += 1;
-            const int s = c->steps;
-            if (s < rc->replay_end && s < rc->record_cap) {
-                c->max_dt = step_dt[s];
+        if (r.replay) {
+            if (cl.active) cl.steps += 1;
+            const int s = cl.steps;
+            if (s < r.replay_end && s < r.record_cap) {
+                cl.max_dt = step_dt[s];
                 s_level = step_code[s] >> 1;
                 red[0] = 0u;
                 red[1] = 0u;
                 red[2] = 0u;
-                c->active = 1;
+                cl.active = 1;
             } else {
-                c->active = 0;
+                cl.active = 0;
             }
         } else {
-            if (c->active) {
-                const uint32_t st = red[2];
-                const float dt = __uint_as_float(red[3]);
+            if (cl.active) {
+                const uint32_t st = red_status;
+                const float dt = __uint_as_float(red_dt);
                 if (st & (SWE_S_NONFINITE_STATE | SWE_S_NONFINITE_DT | SWE_S_NONPOSITIVE_DT)) {
-                    c->state = SWE_CLOCK_FAILED;
-                    c->dt_status = st;
-                    c->last_dt = dt;
+                    cl.state = SWE_CLOCK_FAILED;
+                    cl.dt_status = st;
+                    cl.last_dt = dt;
                 } else {
-                    double elapsed = c->elapsed + (double)dt;
-                    if (elapsed > c->duration && elapsed - c->duration <= c->tolerance)
-                        elapsed = c->duration;
-                    c->last_dt = dt;
-                    const int s = c->steps;
-                    const bool ends = c->duration - elapsed <= c->tolerance;
-                    if (s < rc->record_cap) {
+                    double elapsed = cl.elapsed + (double)dt;
+                    if (elapsed > cl.duration && elapsed - cl.duration <= cl.tolerance)
+                        elapsed = cl.duration;
+                    cl.last_dt = dt;
+                    const int s = cl.steps;
+                    const bool ends = cl.duration - elapsed <= cl.tolerance;
+                    if (s < r.record_cap) {
                         step_dt[s] = dt;
-                        step_code[s] = 2 * rc->chunk + (ends ? 1 : 0);
+                        step_code[s] = 2 * r.chunk + (ends ? 1 : 0);
                     }
-                    c->steps = s + 1;
-                    rc->chunk_steps += 1;
-                    c->elapsed = elapsed;
+                    cl.steps = s + 1;
+                    r.chunk_steps += 1;
+                    cl.elapsed = elapsed;
                     if (ends) {
-                        s_record = rc->chunk;
-                        rc->chunk += 1;
-                        rc->chunk_steps = 0;
-                        c->elapsed = 0.0;
+                        s_record = r.chunk;
+                        r.chunk += 1;
+                        r.chunk_steps = 0;
+                        cl.elapsed = 0.0;
                     }
                 }
             }
-            if (c->state == SWE_CLOCK_RUNNING) {
-                if (rc->chunk >= rc->n_out) {
-                    c->state = SWE_CLOCK_DONE;
-                } else if (c->steps >= rc->record_cap) {
-                    c->state = SWE_CLOCK_RECORD_FULL;
-                } else if (rc->chunk_steps >= c->max_steps) {
-                    c->state = SWE_CLOCK_MAXSTEPS;
+            if (cl.state == SWE_CLOCK_RUNNING) {
+                if (r.chunk >= r.n_out) {
+                    cl.state = SWE_CLOCK_DONE;
+                } else if (cl.steps >= r.record_cap) {
+                    cl.state = SWE_CLOCK_RECORD_FULL;
+                } else if (r.chunk_steps >= cl.max_steps) {
+                    cl.state = SWE_CLOCK_MAXSTEPS;
                 } else {
                     // An interval that has not ended has remaining > tolerance.
-                    const double remaining = c->duration - c->elapsed;
+                    const double remaining = cl.duration - cl.elapsed;
                     double step_max_dt = remaining;
-                    if (c->max_dt_cap > 0.0 && c->max_dt_cap < remaining) step_max_dt = c->max_dt_cap;
-                    c->max_dt = (float)step_max_dt;
-                    s_level = rc->chunk;
+                    if (cl.max_dt_cap > 0.0 && cl.max_dt_cap < remaining) step_max_dt = cl.max_dt_cap;
+                    cl.max_dt = (float)step_max_dt;
+                    s_level = r.chunk;
                     red[0] = 0u;
                     red[1] = 0u;
                     red[2] = 0u;
                 }
             }
-            c->active = c->state == SWE_CLOCK_RUNNING ? 1 : 0;
+            cl.active = cl.state == SWE_CLOCK_RUNNING ? 1 : 0;
         }
+        *rc = r;
     }
     __syncthreads();
     const int rec = s_record, lev = s_level;
