@@ -294,3 +294,54 @@ def test_step_raises_like_reference():
         m.step(U, 0.0, 1.0)
     with pytest.raises(ValueError):
         m.step(torch.zeros(1, 2, 8, 8, device=DEV), 0.0, 1.0)
+
+
+@pytest.mark.parametrize("arithmetic", ["exact", "fast"])
+def test_clocked_step_writes_its_stage2_tendency(golden, arithmetic):
+    """swe_step_clocked_k2_f32: the step equals swe_step_clocked_f32's bit for
+    bit, and k2_out holds the stage-2 tendency -- in the IEEE mode bit for bit
+    the spatial operator at the predictor clean(U, U + dt/2 k1)."""
+    from diffswe2d_b200 import _native as nat
+    d, m = _runup_model(golden)
+    m.arithmetic = arithmetic
+    lib, st, p = nat.lib(), nat.stream_handle(torch.device(DEV)), m._params()
+    U = _t(d["f32cr_200"])
+    B, _, ny, nx = U.shape
+    bed, n = m._fields(U)
+    lv = torch.tensor([0.01], device=DEV)
+
+    def step(with_k2):
+        clock = torch.frombuffer(bytearray(bytes(nat.SweClock(1.0, 0.0, 1e-12, 0.0, 0.0, 10, 0, 0, 0, 0,
+                                                              0.0, 0.0, 0.0))),
+                                 dtype=torch.uint8).to(DEV)
+        red = torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=DEV)
+        k1, out, k2 = torch.empty_like(U), torch.empty_like(U), torch.full_like(U, float("nan"))
+        nat.check(lib.swe_clock_f32(nat.ptr(clock), nat.ptr(red), None, None, 0, nat.ptr(lv), nat.ptr(U),
+                                    ny, nx, None, 0, None, 0, st), "clock")
+        args = (3, nat.ptr(U), nat.ptr(bed), bed.shape[0], nat.ptr(n), n.shape[0], B, ny, nx, p,
+                nat.ptr(lv), 1, nat.ptr(clock), None, nat.FORCING_NONE, 1, nat.ptr(k1), nat.ptr(red),
+                nat.ptr(out), None)
+        if with_k2:
+            nat.check(lib.swe_step_clocked_k2_f32(*args, nat.ptr(k2), st), "step with k2")
+        else:
+            nat.check(lib.swe_step_clocked_f32(*args, st), "step")
+        torch.cuda.synchronize()
+        dt = float(red[3:4].view(torch.float32).item())
+        return out, k1, k2, dt
+
+    out_a, k1_a, k2, dt = step(True)
+    out_b, k1_b, _, dt_b = step(False)
+    assert dt == dt_b and torch.equal(out_a, out_b) and torch.equal(k1_a, k1_b)
+    assert bool(torch.isfinite(k2).all())
+    P = torch.empty_like(U)
+    nat.check(lib.swe_adj_pointwise_f32(2, nat.ptr(U), nat.ptr(k1_a), None, 1, B, ny, nx, p, dt, None, None,
+                                        None, None, nat.ptr(P), st), "predictor")
+    ref, red2 = torch.empty_like(U), torch.zeros(nat.RED_WORDS, dtype=torch.int32, device=DEV)
+    nat.check(lib.swe_spatial_operator_f32(nat.ptr(P), nat.ptr(bed), B, bed.shape[0], ny, nx, p, nat.ptr(lv),
+                                           1, None, nat.FORCING_NONE, 1, None, nat.FORCING_NONE, 1,
+                                           nat.ptr(ref), nat.ptr(red2), st), "k2 at P")
+    torch.cuda.synchronize()
+    if arithmetic == "exact":
+        assert torch.equal(k2, ref)
+    else:
+        assert normwise(_np(k2), _np(ref)) <= 1e-5
