@@ -31,7 +31,7 @@ class SWE2D(nn.Module):
     ``arithmetic`` (not in the reference) selects the step kernels: "exact"
     evaluates every float32 operation of the reference's step in its order
     with IEEE rounding; "fast" is the tolerance mode (fused multiply-adds,
-    hardware approximations, about three times the throughput), within FP32
+    hardware approximations, about twice the throughput), within FP32
     rounding of the reference.  ``rainfall`` is an object with
     ``at(time) -> rate`` (``RainfallForcing``); as in the reference, stage 1
     of a step uses the rate at the step's start and stage 2 the rate half a
@@ -553,6 +553,22 @@ class SWE2D(nn.Module):
             self.ts_z[name].append(depth + bed)
 
 
+def replay_lengths(chunk: int):
+    """Step counts of the device loop's graphs: ``chunk`` and its halvings
+    while they stay even (32 -> [32, 16, 8, 4, 2]); every length is even so
+    that a replay leaves the state in the first of the two buffers."""
+    sizes = [int(chunk)]
+    while sizes[-1] > 2 and sizes[-1] % 4 == 0:
+        sizes.append(sizes[-1] // 2)
+    return sizes
+
+
+def replay_length(sizes, left: float) -> int:
+    """The longest of ``sizes`` (descending) that ``left`` more steps fill,
+    else the shortest."""
+    return next((m for m in sizes if m <= left), sizes[-1])
+
+
 class _DeviceLoop:
     """Buffers and captured CUDA graph of the device-driven forward() loop for
     one (shape, configuration) of a model.  Inputs are copied into the
@@ -587,9 +603,7 @@ class _DeviceLoop:
         # to 2): near the end of a call the host replays the longest one that
         # the remaining time still fills, so that few steps run inactive
         # (an inactive step still copies the state through)
-        self.sizes = [self.chunk]
-        while self.sizes[-1] > 2 and self.sizes[-1] % 4 == 0:
-            self.sizes.append(self.sizes[-1] // 2)
+        self.sizes = replay_lengths(self.chunk)
         self.graphs = {}
         self.dt_hint = 0.0  # mean step of the calls so far (sizes a call's first replay)
 
@@ -638,8 +652,8 @@ class _DeviceLoop:
                         for s in range(n):
                             self._step(self.bufs[s % 2], self.bufs[1 - s % 2])
                     self.graphs[n] = graph
-        def size_for(left):  # the longest graph that `left` more steps fill
-            return next((m for m in self.sizes if m <= left), self.sizes[-1])
+        def size_for(left):
+            return replay_length(self.sizes, left)
 
         n = size_for(clock.duration / self.dt_hint) if self.dt_hint > 0 else self.chunk
         while True:
