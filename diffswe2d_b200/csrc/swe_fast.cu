@@ -15,7 +15,7 @@
 //   * algebraic identities of the reference's expressions are used where
 //     they save work: a face's velocity (h_cn u)/h_cn is u itself, the
 //     limiter's centred difference is the sum of the two one-sided ones,
-//     minmod3 is max(min(a,b,c), 0) + min(max(a,b,c), 0), the positivity
+//     minmod3 is max(min(a,b,c), min(max(a,b,c), 0)), the positivity
 //     limiter scales the increment dt*k directly;
 //   * the one-sided differences along y are carried from row to row, those
 //     along x exchanged with one shuffle per field; the x-direction part of
